@@ -1,0 +1,212 @@
+/*
+ * rsgpu.h -- C ABI of the B200 erasure-coding library (librsgpu.so).
+ *
+ * The library replaces the encode / reconstruct / verify hot path of
+ * rustfs-erasure-codec 9.1.0 (a Rust crate with no C ABI of its own).  Every
+ * entry point below names the reference API it stands in for (file:line in
+ * the reference crate); a Rust binding maps each `ReedSolomon` method onto one
+ * call.
+ *
+ * Conventions
+ *  - Return value: 0 on success, otherwise the reference `Error` discriminant
+ *    + 1 (src/errors.rs:3-21, values 1..16 below), or a device/runtime code
+ *    (>= 100).  Every argument check runs on the host before any launch, so a
+ *    call that fails validation writes nothing.
+ *  - Shards are passed as arrays of pointers plus an array of per-shard byte
+ *    lengths, the flat equivalent of the reference's `&[T: AsRef<[u8]>]`.
+ *    `mem` says where the bytes live: RSGPU_MEM_HOST (pageable or pinned host
+ *    memory; the library stages it through device memory and the call returns
+ *    once results are back in host memory) or RSGPU_MEM_DEVICE (device memory
+ *    of the codec's GPU; work is queued on `stream` and the call returns
+ *    without waiting, except where a host-visible result such as a verify
+ *    flag is returned).
+ *  - `stream` is a cudaStream_t passed as void* (NULL = the legacy default
+ *    stream).
+ *  - A codec handle may be shared by threads; its caches are internally
+ *    locked.  Workspaces belong to one caller at a time.
+ */
+#ifndef RSGPU_H
+#define RSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes (src/errors.rs:3-21, discriminant + 1) ---- */
+enum {
+  RSGPU_OK = 0,
+  RSGPU_ERR_TOO_FEW_SHARDS = 1,
+  RSGPU_ERR_TOO_MANY_SHARDS = 2,
+  RSGPU_ERR_TOO_FEW_DATA_SHARDS = 3,
+  RSGPU_ERR_TOO_MANY_DATA_SHARDS = 4,
+  RSGPU_ERR_TOO_FEW_PARITY_SHARDS = 5,
+  RSGPU_ERR_TOO_MANY_PARITY_SHARDS = 6,
+  RSGPU_ERR_TOO_FEW_BUFFER_SHARDS = 7,
+  RSGPU_ERR_TOO_MANY_BUFFER_SHARDS = 8,
+  RSGPU_ERR_INCORRECT_SHARD_SIZE = 9,
+  RSGPU_ERR_TOO_FEW_SHARDS_PRESENT = 10,
+  RSGPU_ERR_EMPTY_SHARD = 11,
+  RSGPU_ERR_INVALID_SHARD_FLAGS = 12,
+  RSGPU_ERR_INVALID_INDEX = 13,
+  RSGPU_ERR_INVALID_CUSTOM_MATRIX = 14,
+  RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY = 15,
+  RSGPU_ERR_UNSUPPORTED_LEOPARD_PROTOTYPE = 16,
+  /* device / runtime conditions with no reference counterpart */
+  RSGPU_ERR_CUDA = 100,
+  RSGPU_ERR_OUT_OF_MEMORY = 101,
+  RSGPU_ERR_INVALID_ARGUMENT = 102,
+  RSGPU_ERR_DEVICE_TIMEOUT = 103,
+  RSGPU_ERR_NO_DEVICE = 104,
+};
+
+enum { RSGPU_MEM_HOST = 0, RSGPU_MEM_DEVICE = 1 };
+
+/* src/core/options.rs:14-82 */
+enum { RSGPU_FAMILY_CLASSIC = 0, RSGPU_FAMILY_LEOPARD_GF8 = 1, RSGPU_FAMILY_LEOPARD_GF16 = 2 };
+enum {
+  RSGPU_LEOPARD_DISABLED = 0,
+  RSGPU_LEOPARD_AS_NEEDED = 1,
+  RSGPU_LEOPARD_PREFER_GF16 = 2,
+  RSGPU_LEOPARD_PREFER_LEOPARD = 3
+};
+enum {
+  RSGPU_MATRIX_VANDERMONDE = 0,
+  RSGPU_MATRIX_CAUCHY = 1,
+  RSGPU_MATRIX_JERASURE_LIKE = 2,
+  RSGPU_MATRIX_CUSTOM = 3
+};
+/* src/core/recovery_plan.rs:11-16 (ReconstructionGoal) */
+enum { RSGPU_GOAL_ALL = 0, RSGPU_GOAL_DATA = 1, RSGPU_GOAL_REQUIRED = 2 };
+/* Field of a classic codec: galois_8 (bytes) or galois_16 (2-byte tower). */
+enum { RSGPU_FIELD_GF8 = 0, RSGPU_FIELD_GF16_TOWER = 1 };
+
+/* src/core/options.rs:97-146 (CodecOptions).  Zero means "automatic" exactly
+ * as in the reference. */
+typedef struct rsgpu_options {
+  int32_t fast_one_parity;
+  int32_t inversion_cache;
+  size_t inversion_cache_capacity;
+  size_t inversion_cache_max_bytes;
+  int32_t codec_family;
+  int32_t leopard_mode;
+  int32_t matrix_mode;
+  size_t max_parallel_jobs;
+} rsgpu_options;
+
+typedef struct rsgpu_codec rsgpu_codec;
+typedef struct rsgpu_verify_ws rsgpu_verify_ws;
+typedef struct rsgpu_reconstruct_ws rsgpu_reconstruct_ws;
+
+/* Cache statistics (src/core/metrics.rs:105-215, ReconstructionCacheStats). */
+typedef struct rsgpu_cache_stats {
+  uint64_t requests, hits, misses, inserts, evictions;
+  uint64_t entries, retained_bytes;
+} rsgpu_cache_stats;
+
+/* ------------------------------------------------------------ construction */
+/* src/core/options.rs:134-146 (CodecOptions::default). */
+void rsgpu_options_default(rsgpu_options *out);
+
+/* src/core/codec.rs:264-349 (ReedSolomon::new / with_options), galois_8. */
+int32_t rsgpu_codec_new(size_t data_shards, size_t parity_shards, const rsgpu_options *opts,
+                        rsgpu_codec **out);
+/* src/core/codec.rs:546-615 (with_custom_matrix); rows = parity_shards rows
+ * of data_shards coefficients, row-major. */
+int32_t rsgpu_codec_with_custom_matrix(size_t data_shards, size_t parity_shards,
+                                       const uint8_t *rows, const rsgpu_options *opts,
+                                       rsgpu_codec **out);
+/* src/galois_16.rs:605 (galois_16::ReedSolomon::new): classic codec over the
+ * GF((2^8)^2) tower field; shard lengths count bytes and must be even. */
+int32_t rsgpu_codec_new_gf16(size_t data_shards, size_t parity_shards, rsgpu_codec **out);
+void rsgpu_codec_free(rsgpu_codec *codec);
+
+/* src/core/codec.rs:353-380 (data_shard_count, parity_shard_count, ...) */
+size_t rsgpu_data_shard_count(const rsgpu_codec *codec);
+size_t rsgpu_parity_shard_count(const rsgpu_codec *codec);
+size_t rsgpu_total_shard_count(const rsgpu_codec *codec);
+int32_t rsgpu_codec_family(const rsgpu_codec *codec);
+/* Classic encoding matrix, (k+m)*k coefficients (2 bytes each for the tower
+ * field); src/core/format.rs matrix rows.  Returns
+ * RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY for Leopard codecs. */
+int32_t rsgpu_encoding_matrix(const rsgpu_codec *codec, uint8_t *out, size_t out_len);
+
+/* ------------------------------------------------------------ per-call API */
+/* src/core/encode.rs:935-947 (encode): shards[0..k) are read, shards[k..k+m)
+ * are written. */
+int32_t rsgpu_encode(const rsgpu_codec *codec, uint8_t *const *shards, const size_t *lens,
+                     size_t n_shards, int32_t mem, void *stream);
+/* src/core/encode.rs:950-972 (encode_sep). */
+int32_t rsgpu_encode_sep(const rsgpu_codec *codec, const uint8_t *const *data,
+                         const size_t *data_lens, size_t n_data, uint8_t *const *parity,
+                         const size_t *parity_lens, size_t n_parity, int32_t mem, void *stream);
+/* src/core/reconstruct.rs:731-790 (reconstruct / reconstruct_data /
+ * reconstruct_some).  present[i] == 0 marks shard i missing; a missing shard
+ * must still point at a writable buffer of the common length when it is a
+ * target.  `lens[i]` is ignored for missing shards.  For
+ * RSGPU_GOAL_REQUIRED, `required` holds n_required flags (k or k+m). */
+int32_t rsgpu_reconstruct(const rsgpu_codec *codec, uint8_t *const *shards, const size_t *lens,
+                          const uint8_t *present, size_t n_shards, int32_t goal,
+                          const uint8_t *required, size_t n_required, int32_t mem,
+                          void *stream);
+/* src/core/verify.rs:72-94 (verify).  *ok receives 1 or 0. */
+int32_t rsgpu_verify(const rsgpu_codec *codec, const uint8_t *const *shards, const size_t *lens,
+                     size_t n_shards, int32_t *ok, int32_t mem, void *stream);
+
+/* src/core/workspace.rs:16-69 (VerifyWorkspace) and src/core/verify.rs:96-115
+ * (verify_with_workspace).  The workspace keeps the device staging and the
+ * mismatch flag between calls. */
+int32_t rsgpu_verify_ws_new(const rsgpu_codec *codec, size_t shard_len, rsgpu_verify_ws **out);
+void rsgpu_verify_ws_free(rsgpu_verify_ws *ws);
+int32_t rsgpu_verify_with_workspace(const rsgpu_codec *codec, const uint8_t *const *shards,
+                                    const size_t *lens, size_t n_shards, rsgpu_verify_ws *ws,
+                                    int32_t *ok, int32_t mem, void *stream);
+
+/* src/core/reconstruct.rs:539-726 (prepare_reconstruct_workspace /
+ * reconstruct_with_workspace): a reusable plan for one erasure pattern. */
+int32_t rsgpu_prepare_reconstruct_ws(const rsgpu_codec *codec, const uint8_t *present,
+                                     size_t n_shards, size_t shard_len, int32_t goal,
+                                     const uint8_t *required, size_t n_required,
+                                     rsgpu_reconstruct_ws **out);
+void rsgpu_reconstruct_ws_free(rsgpu_reconstruct_ws *ws);
+/* Targets of a prepared plan (src/core/workspace.rs:92-112). */
+size_t rsgpu_reconstruct_ws_targets(const rsgpu_reconstruct_ws *ws, size_t *out, size_t cap);
+int32_t rsgpu_reconstruct_with_ws(const rsgpu_codec *codec, rsgpu_reconstruct_ws *ws,
+                                  uint8_t *const *shards, const size_t *lens,
+                                  const uint8_t *present, size_t n_shards, int32_t mem,
+                                  void *stream);
+
+/* ------------------------------------------------------------ batched API */
+/* Many stripes of one codec and one shard length in a single launch (no
+ * reference counterpart: the reference codes one stripe per call).
+ * shard_ptrs holds n_stripes * (k+m) pointers, stripe-major, all in `mem`.
+ * src/core/encode.rs:950-972 semantics per stripe. */
+int32_t rsgpu_encode_batch(const rsgpu_codec *codec, size_t n_stripes, uint8_t *const *shard_ptrs,
+                           size_t shard_len, int32_t mem, void *stream);
+/* Per-stripe erasure patterns: present holds n_stripes * (k+m) flags.
+ * src/core/reconstruct.rs:731-790 semantics per stripe. */
+int32_t rsgpu_reconstruct_batch(const rsgpu_codec *codec, size_t n_stripes,
+                                uint8_t *const *shard_ptrs, const uint8_t *present,
+                                size_t shard_len, int32_t goal, int32_t mem, void *stream);
+/* ok receives n_stripes flags (host memory).  src/core/verify.rs:72-94. */
+int32_t rsgpu_verify_batch(const rsgpu_codec *codec, size_t n_stripes,
+                           const uint8_t *const *shard_ptrs, size_t shard_len, uint8_t *ok,
+                           int32_t mem, void *stream);
+
+/* ------------------------------------------------------------ introspection */
+/* src/core/codec.rs:412-414 (reconstruction_cache_stats): device decode-table
+ * cache of this codec. */
+int32_t rsgpu_get_cache_stats(const rsgpu_codec *codec, rsgpu_cache_stats *out);
+/* Number of kernels this process launched through the library so far. */
+uint64_t rsgpu_kernel_launch_count(void);
+/* Human-readable text for a return code. */
+const char *rsgpu_error_string(int32_t code);
+/* Library build identification ("rsgpu <version> sm_100a"). */
+const char *rsgpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RSGPU_H */

@@ -1,0 +1,537 @@
+// capi.cpp -- the extern "C" boundary (include/rsgpu.h).
+//
+// Each entry point validates its arguments with the reference's error
+// precedence (src/macros.rs:142-245, src/core/recovery_plan.rs:262-387,
+// src/core/reconstruct.rs:795-838) before any device work, then hands device
+// pointers to the Codec.  Host-memory calls are staged through device memory
+// in chunks on two internal streams so that the host->device copy of one
+// chunk overlaps the kernels and device->host copy of the previous one.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "codec.hpp"
+#include "leopard.hpp"
+#include "rsgpu.h"
+
+using rsgpu::Codec;
+
+struct rsgpu_codec {
+  Codec c;
+  // internal streams for host-memory staging
+  cudaStream_t io[2] = {nullptr, nullptr};
+  std::mutex io_mu;
+};
+
+struct rsgpu_verify_ws {
+  size_t shard_len = 0;
+};
+
+struct rsgpu_reconstruct_ws {
+  std::vector<uint8_t> present;
+  size_t shard_len = 0;
+  int goal = 0;
+  std::vector<uint8_t> required;
+  std::vector<size_t> targets;
+};
+
+namespace rsgpu {
+uint64_t launch_counter();
+}
+
+namespace {
+
+#define RS_CUDA(expr)                                 \
+  do {                                                \
+    cudaError_t e_ = (expr);                          \
+    if (e_ != cudaSuccess) return rsgpu::cuda_status(e_); \
+  } while (0)
+
+inline cudaStream_t S(void *p) { return static_cast<cudaStream_t>(p); }
+
+int ensure_io(rsgpu_codec *h) {
+  if (!h->io[0]) {
+    RS_CUDA(cudaStreamCreateWithFlags(&h->io[0], cudaStreamNonBlocking));
+    RS_CUDA(cudaStreamCreateWithFlags(&h->io[1], cudaStreamNonBlocking));
+  }
+  return RSGPU_OK;
+}
+
+size_t round16(size_t n) { return (n + 15) & ~size_t(15); }
+
+// Stripes per host-staging chunk: about 256 MiB of device staging each.
+size_t chunk_stripes(size_t per_stripe_bytes) {
+  size_t c = (256u << 20) / std::max<size_t>(per_stripe_bytes, 1);
+  return std::max<size_t>(c, 1);
+}
+
+int new_codec(size_t k, size_t m, const rsgpu_options *opts, const uint8_t *custom, int field,
+              rsgpu_codec **out) {
+  if (!out) return RSGPU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  rsgpu_options o;
+  rsgpu_options_default(&o);
+  if (opts) o = *opts;
+  // src/core/codec.rs:269-349 (with_options) check order.
+  if (k == 0) return RSGPU_ERR_TOO_FEW_DATA_SHARDS;
+  if (m == 0) return RSGPU_ERR_TOO_FEW_PARITY_SHARDS;
+  const size_t total = k + m;
+  if (custom) {
+    if (total > 256) return RSGPU_ERR_TOO_MANY_SHARDS;
+    if (o.codec_family != RSGPU_FAMILY_CLASSIC) return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY;
+    o.matrix_mode = RSGPU_MATRIX_CUSTOM;
+  } else if (field == RSGPU_FIELD_GF8) {
+    o.codec_family = rsgpu::resolve_family(o.codec_family, o.leopard_mode, total, m);
+    const size_t cap = o.codec_family == RSGPU_FAMILY_LEOPARD_GF16 ? 65536 : 256;
+    if (total > cap) return RSGPU_ERR_TOO_MANY_SHARDS;
+    int rc = rsgpu::validate_leopard_family(o.codec_family, k, m);
+    if (rc) return rc;
+    if (o.codec_family == RSGPU_FAMILY_CLASSIC && o.matrix_mode == RSGPU_MATRIX_CUSTOM)
+      return RSGPU_ERR_INVALID_CUSTOM_MATRIX;
+  } else {
+    if (total > 65536) return RSGPU_ERR_TOO_MANY_SHARDS;
+    if (o.codec_family != RSGPU_FAMILY_CLASSIC) return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RSGPU_ERR_NO_DEVICE;
+  rsgpu_codec *h = new (std::nothrow) rsgpu_codec();
+  if (!h) return RSGPU_ERR_OUT_OF_MEMORY;
+  Codec &c = h->c;
+  c.k = k;
+  c.m = m;
+  c.opts = o;
+  c.family = o.codec_family;
+  c.field = field;
+  int rc;
+  if (field == RSGPU_FIELD_GF16_TOWER)
+    rc = c.init_tower();
+  else if (c.family == RSGPU_FAMILY_CLASSIC)
+    rc = c.init_classic(custom);
+  else
+    rc = c.init_leopard();
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return RSGPU_OK;
+}
+
+// ---------------------------------------------------------------- dispatch
+// Device-pointer operations for any family.
+int do_encode(Codec &c, size_t n, uint8_t *const *sh, size_t len, cudaStream_t s) {
+  if (c.family != RSGPU_FAMILY_CLASSIC) return rsgpu::leopard_encode(c, n, sh, len, s);
+  if (c.field == RSGPU_FIELD_GF16_TOWER) return rsgpu::tower_encode(c, n, sh, len, s);
+  return c.encode_dev(n, sh, len, s);
+}
+int do_verify(Codec &c, size_t n, const uint8_t *const *sh, size_t len, uint8_t *ok, cudaStream_t s) {
+  if (c.family != RSGPU_FAMILY_CLASSIC) return rsgpu::leopard_verify(c, n, sh, len, ok, s);
+  if (c.field == RSGPU_FIELD_GF16_TOWER) return rsgpu::tower_verify(c, n, sh, len, ok, s);
+  return c.verify_dev(n, sh, len, ok, s);
+}
+int do_reconstruct(Codec &c, size_t n, uint8_t *const *sh, const uint8_t *present, size_t len, int goal,
+                   const uint8_t *req, size_t nreq, cudaStream_t s) {
+  if (c.family != RSGPU_FAMILY_CLASSIC) return rsgpu::leopard_reconstruct(c, n, sh, present, len, goal, req, nreq, s);
+  if (c.field == RSGPU_FIELD_GF16_TOWER)
+    return rsgpu::tower_reconstruct(c, n, sh, present, len, goal, req, nreq, s);
+  return c.reconstruct_dev(n, sh, present, len, goal, req, nreq, s);
+}
+
+// Which shards a stripe reads (in) and writes (out) for an operation.
+enum Op { OP_ENCODE, OP_VERIFY, OP_RECONSTRUCT };
+
+// Host-memory execution: stage chunks of stripes through device memory.
+// `in_mask`/`out_mask` (per stripe, k+m flags) say which shards to copy in
+// and back.
+int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, const uint8_t *present, size_t len,
+             int goal, const uint8_t *req, size_t nreq, uint8_t *ok, void *user_stream) {
+  Codec &c = h->c;
+  const size_t total = c.k + c.m;
+  std::lock_guard<std::mutex> g(h->io_mu);
+  int rc = ensure_io(h);
+  if (rc) return rc;
+  // Order after work already queued on the caller's stream.
+  cudaEvent_t ev;
+  RS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  RS_CUDA(cudaEventRecord(ev, S(user_stream)));
+  RS_CUDA(cudaStreamWaitEvent(h->io[0], ev, 0));
+  RS_CUDA(cudaStreamWaitEvent(h->io[1], ev, 0));
+  cudaEventDestroy(ev);
+  const size_t pitch = round16(len);
+  const size_t per = chunk_stripes(total * pitch);
+  std::vector<uint8_t *> dptr;
+  std::vector<uint8_t> in_flags(total), out_flags(total);
+  int status = RSGPU_OK;
+  for (size_t base = 0, ci = 0; base < n_stripes && status == RSGPU_OK; base += per, ++ci) {
+    const size_t cnt = std::min(per, n_stripes - base);
+    cudaStream_t s = h->io[ci & 1];
+    uint8_t *stage = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&stage), cnt * total * pitch, s);
+    if (e != cudaSuccess) return rsgpu::cuda_status(e);
+    dptr.resize(cnt * total);
+    for (size_t i = 0; i < cnt * total; ++i) dptr[i] = stage + i * pitch;
+    // Inputs first so the codec's metadata upload (queued after) does not wait on them.
+    for (size_t sidx = 0; sidx < cnt; ++sidx) {
+      const size_t st = base + sidx;
+      for (size_t i = 0; i < total; ++i) {
+        bool in = op == OP_ENCODE ? i < c.k : op == OP_VERIFY ? true : present[st * total + i] != 0;
+        if (in)
+          RS_CUDA(cudaMemcpyAsync(dptr[sidx * total + i], host[st * total + i], len, cudaMemcpyHostToDevice, s));
+      }
+    }
+    if (op == OP_ENCODE)
+      status = do_encode(c, cnt, dptr.data(), len, s);
+    else if (op == OP_VERIFY)
+      status = do_verify(c, cnt, const_cast<const uint8_t *const *>(dptr.data()), len, ok + base, s);
+    else
+      status = do_reconstruct(c, cnt, dptr.data(), present + base * total, len, goal, req, nreq, s);
+    if (status == RSGPU_OK && op != OP_VERIFY) {
+      for (size_t sidx = 0; sidx < cnt; ++sidx) {
+        const size_t st = base + sidx;
+        const uint8_t *pr = op == OP_RECONSTRUCT ? present + st * total : nullptr;
+        // Which missing shards are targets follows the goal.
+        for (size_t i = 0; i < total; ++i) {
+          bool out;
+          if (op == OP_ENCODE)
+            out = i >= c.k;
+          else {
+            out = !pr[i] && (goal == RSGPU_GOAL_ALL || (goal == RSGPU_GOAL_DATA && i < c.k) ||
+                             (goal == RSGPU_GOAL_REQUIRED && i < nreq && req[i]));
+          }
+          if (out)
+            RS_CUDA(cudaMemcpyAsync(host[st * total + i], dptr[sidx * total + i], len, cudaMemcpyDeviceToHost, s));
+        }
+      }
+    }
+    RS_CUDA(cudaFreeAsync(stage, s));
+  }
+  RS_CUDA(cudaStreamSynchronize(h->io[0]));
+  RS_CUDA(cudaStreamSynchronize(h->io[1]));
+  return status;
+}
+
+// Per-call shard validation for reconstruct (src/core/recovery_plan.rs:262-387).
+int check_reconstruct(const Codec &c, const size_t *lens, const uint8_t *present, size_t n, int goal,
+                      const uint8_t *required, size_t n_required, size_t *shard_len) {
+  const size_t total = c.k + c.m;
+  if (goal == RSGPU_GOAL_REQUIRED && n_required != c.k && n_required != total) return RSGPU_ERR_INVALID_SHARD_FLAGS;
+  if (n < total) return RSGPU_ERR_TOO_FEW_SHARDS;
+  if (n > total) return RSGPU_ERR_TOO_MANY_SHARDS;
+  size_t len = 0, np = 0;
+  const bool leopard = c.family != RSGPU_FAMILY_CLASSIC;
+  for (size_t i = 0; i < n; ++i) {
+    if (!present[i]) continue;
+    if (lens[i] == 0) return RSGPU_ERR_EMPTY_SHARD;
+    if ((len && lens[i] != len) || (leopard && lens[i] % 64)) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+    len = lens[i];
+    ++np;
+  }
+  if (np < c.k) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+  if (np == total) {
+    *shard_len = 0;  // nothing to do
+    return RSGPU_OK;
+  }
+  if (c.field == RSGPU_FIELD_GF16_TOWER && len % 2) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  // A missing target must come with a buffer of the shard length (ShardSlot
+  // semantics, src/lib.rs:377-406).
+  for (size_t i = 0; i < n; ++i) {
+    if (present[i]) continue;
+    bool target = goal == RSGPU_GOAL_ALL || (goal == RSGPU_GOAL_DATA && i < c.k) ||
+                  (goal == RSGPU_GOAL_REQUIRED && i < n_required && required[i]);
+    if (target && lens[i] < len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  }
+  *shard_len = len;
+  return RSGPU_OK;
+}
+
+int check_family_len(const Codec &c, size_t len) {
+  if (c.family != RSGPU_FAMILY_CLASSIC && (len % 64)) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  if (c.field == RSGPU_FIELD_GF16_TOWER && (len % 2)) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  return RSGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void rsgpu_options_default(rsgpu_options *out) {
+  if (!out) return;
+  std::memset(out, 0, sizeof(*out));
+  out->inversion_cache = 1;
+  out->codec_family = RSGPU_FAMILY_CLASSIC;
+  out->leopard_mode = RSGPU_LEOPARD_DISABLED;
+  out->matrix_mode = RSGPU_MATRIX_VANDERMONDE;
+}
+
+int32_t rsgpu_codec_new(size_t k, size_t m, const rsgpu_options *opts, rsgpu_codec **out) {
+  return new_codec(k, m, opts, nullptr, RSGPU_FIELD_GF8, out);
+}
+
+int32_t rsgpu_codec_with_custom_matrix(size_t k, size_t m, const uint8_t *rows, const rsgpu_options *opts,
+                                       rsgpu_codec **out) {
+  if (!rows) return RSGPU_ERR_INVALID_CUSTOM_MATRIX;
+  return new_codec(k, m, opts, rows, RSGPU_FIELD_GF8, out);
+}
+
+int32_t rsgpu_codec_new_gf16(size_t k, size_t m, rsgpu_codec **out) {
+  return new_codec(k, m, nullptr, nullptr, RSGPU_FIELD_GF16_TOWER, out);
+}
+
+void rsgpu_codec_free(rsgpu_codec *h) {
+  if (!h) return;
+  if (h->io[0]) {
+    cudaStreamSynchronize(h->io[0]);
+    cudaStreamSynchronize(h->io[1]);
+    cudaStreamDestroy(h->io[0]);
+    cudaStreamDestroy(h->io[1]);
+  }
+  delete h;
+}
+
+size_t rsgpu_data_shard_count(const rsgpu_codec *h) { return h ? h->c.k : 0; }
+size_t rsgpu_parity_shard_count(const rsgpu_codec *h) { return h ? h->c.m : 0; }
+size_t rsgpu_total_shard_count(const rsgpu_codec *h) { return h ? h->c.k + h->c.m : 0; }
+int32_t rsgpu_codec_family(const rsgpu_codec *h) { return h ? h->c.family : -1; }
+
+int32_t rsgpu_encoding_matrix(const rsgpu_codec *h, uint8_t *out, size_t out_len) {
+  if (!h || !out) return RSGPU_ERR_INVALID_ARGUMENT;
+  const Codec &c = h->c;
+  if (c.family != RSGPU_FAMILY_CLASSIC) return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY;
+  if (c.field == RSGPU_FIELD_GF16_TOWER) {
+    if (out_len < c.tmatrix.size() * 2) return RSGPU_ERR_INVALID_ARGUMENT;
+    for (size_t i = 0; i < c.tmatrix.size(); ++i) {
+      out[2 * i] = c.tmatrix[i].x;
+      out[2 * i + 1] = c.tmatrix[i].c;
+    }
+    return RSGPU_OK;
+  }
+  if (out_len < c.matrix.size()) return RSGPU_ERR_INVALID_ARGUMENT;
+  std::memcpy(out, c.matrix.data(), c.matrix.size());
+  return RSGPU_OK;
+}
+
+int32_t rsgpu_encode(const rsgpu_codec *hc, uint8_t *const *shards, const size_t *lens, size_t n, int32_t mem,
+                     void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || !shards || !lens) return RSGPU_ERR_INVALID_ARGUMENT;
+  size_t len = 0;
+  int rc = h->c.check_all(lens, n, &len);
+  if (rc) return rc;
+  if ((rc = check_family_len(h->c, len))) return rc;
+  if (mem == RSGPU_MEM_DEVICE) return do_encode(h->c, 1, shards, len, S(stream));
+  return run_host(h, OP_ENCODE, 1, shards, nullptr, len, 0, nullptr, 0, nullptr, stream);
+}
+
+int32_t rsgpu_encode_sep(const rsgpu_codec *hc, const uint8_t *const *data, const size_t *dl, size_t nd,
+                         uint8_t *const *parity, const size_t *pl, size_t np, int32_t mem, void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || !data || !dl || !parity || !pl) return RSGPU_ERR_INVALID_ARGUMENT;
+  const Codec &c = h->c;
+  // check_piece_count!(data), (parity), then check_slices!(multi, multi)
+  // (src/core/encode.rs:955-958).
+  if (nd < c.k) return RSGPU_ERR_TOO_FEW_DATA_SHARDS;
+  if (nd > c.k) return RSGPU_ERR_TOO_MANY_DATA_SHARDS;
+  if (np < c.m) return RSGPU_ERR_TOO_FEW_PARITY_SHARDS;
+  if (np > c.m) return RSGPU_ERR_TOO_MANY_PARITY_SHARDS;
+  if (dl[0] == 0) return RSGPU_ERR_EMPTY_SHARD;
+  for (size_t i = 0; i < nd; ++i)
+    if (dl[i] != dl[0]) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  if (pl[0] == 0) return RSGPU_ERR_EMPTY_SHARD;
+  for (size_t i = 0; i < np; ++i)
+    if (pl[i] != pl[0]) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  if (dl[0] != pl[0]) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  int rc = check_family_len(c, dl[0]);
+  if (rc) return rc;
+  std::vector<uint8_t *> all(c.k + c.m);
+  for (size_t i = 0; i < c.k; ++i) all[i] = const_cast<uint8_t *>(data[i]);
+  for (size_t i = 0; i < c.m; ++i) all[c.k + i] = parity[i];
+  if (mem == RSGPU_MEM_DEVICE) return do_encode(h->c, 1, all.data(), dl[0], S(stream));
+  return run_host(h, OP_ENCODE, 1, all.data(), nullptr, dl[0], 0, nullptr, 0, nullptr, stream);
+}
+
+int32_t rsgpu_verify(const rsgpu_codec *hc, const uint8_t *const *shards, const size_t *lens, size_t n,
+                     int32_t *ok, int32_t mem, void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || !shards || !lens || !ok) return RSGPU_ERR_INVALID_ARGUMENT;
+  size_t len = 0;
+  int rc = h->c.check_all(lens, n, &len);
+  if (rc) return rc;
+  if ((rc = check_family_len(h->c, len))) return rc;
+  uint8_t flag = 0;
+  if (mem == RSGPU_MEM_DEVICE)
+    rc = do_verify(h->c, 1, shards, len, &flag, S(stream));
+  else
+    rc = run_host(h, OP_VERIFY, 1, const_cast<uint8_t *const *>(shards), nullptr, len, 0, nullptr, 0, &flag, stream);
+  if (rc == RSGPU_OK) *ok = flag;
+  return rc;
+}
+
+int32_t rsgpu_verify_ws_new(const rsgpu_codec *h, size_t shard_len, rsgpu_verify_ws **out) {
+  if (!h || !out) return RSGPU_ERR_INVALID_ARGUMENT;
+  rsgpu_verify_ws *w = new (std::nothrow) rsgpu_verify_ws();
+  if (!w) return RSGPU_ERR_OUT_OF_MEMORY;
+  w->shard_len = shard_len;
+  *out = w;
+  return RSGPU_OK;
+}
+
+void rsgpu_verify_ws_free(rsgpu_verify_ws *ws) { delete ws; }
+
+int32_t rsgpu_verify_with_workspace(const rsgpu_codec *h, const uint8_t *const *shards, const size_t *lens, size_t n,
+                                    rsgpu_verify_ws *ws, int32_t *ok, int32_t mem, void *stream) {
+  if (!ws) return RSGPU_ERR_INVALID_ARGUMENT;
+  // The workspace adapts to the call's shard length, as VerifyWorkspace::prepare does.
+  int rc = rsgpu_verify(h, shards, lens, n, ok, mem, stream);
+  if (rc == RSGPU_OK) ws->shard_len = lens[0];
+  return rc;
+}
+
+int32_t rsgpu_reconstruct(const rsgpu_codec *hc, uint8_t *const *shards, const size_t *lens, const uint8_t *present,
+                          size_t n, int32_t goal, const uint8_t *required, size_t n_required, int32_t mem,
+                          void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || !shards || !lens || !present) return RSGPU_ERR_INVALID_ARGUMENT;
+  if (goal == RSGPU_GOAL_REQUIRED && !required) return RSGPU_ERR_INVALID_SHARD_FLAGS;
+  size_t len = 0;
+  int rc = check_reconstruct(h->c, lens, present, n, goal, required, n_required, &len);
+  if (rc || len == 0) return rc;
+  if (mem == RSGPU_MEM_DEVICE) return do_reconstruct(h->c, 1, shards, present, len, goal, required, n_required, S(stream));
+  return run_host(h, OP_RECONSTRUCT, 1, shards, present, len, goal, required, n_required, nullptr, stream);
+}
+
+int32_t rsgpu_prepare_reconstruct_ws(const rsgpu_codec *h, const uint8_t *present, size_t n, size_t shard_len,
+                                     int32_t goal, const uint8_t *required, size_t n_required,
+                                     rsgpu_reconstruct_ws **out) {
+  if (!h || !present || !out) return RSGPU_ERR_INVALID_ARGUMENT;
+  const Codec &c = h->c;
+  const size_t total = c.k + c.m;
+  if (goal == RSGPU_GOAL_REQUIRED && (!required || (n_required != c.k && n_required != total)))
+    return RSGPU_ERR_INVALID_SHARD_FLAGS;
+  if (n < total) return RSGPU_ERR_TOO_FEW_SHARDS;
+  if (n > total) return RSGPU_ERR_TOO_MANY_SHARDS;
+  if (shard_len == 0) return RSGPU_ERR_EMPTY_SHARD;
+  size_t np = 0;
+  for (size_t i = 0; i < n; ++i) np += present[i] ? 1 : 0;
+  if (np < c.k) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+  rsgpu_reconstruct_ws *w = new (std::nothrow) rsgpu_reconstruct_ws();
+  if (!w) return RSGPU_ERR_OUT_OF_MEMORY;
+  w->present.assign(present, present + n);
+  w->shard_len = shard_len;
+  w->goal = goal;
+  if (goal == RSGPU_GOAL_REQUIRED) w->required.assign(required, required + n_required);
+  for (size_t i = 0; i < n; ++i) {
+    if (present[i]) continue;
+    bool t = goal == RSGPU_GOAL_ALL || (goal == RSGPU_GOAL_DATA && i < c.k) ||
+             (goal == RSGPU_GOAL_REQUIRED && i < n_required && required[i]);
+    if (t) w->targets.push_back(i);
+  }
+  *out = w;
+  return RSGPU_OK;
+}
+
+void rsgpu_reconstruct_ws_free(rsgpu_reconstruct_ws *ws) { delete ws; }
+
+size_t rsgpu_reconstruct_ws_targets(const rsgpu_reconstruct_ws *ws, size_t *out, size_t cap) {
+  if (!ws) return 0;
+  for (size_t i = 0; i < ws->targets.size() && i < cap && out; ++i) out[i] = ws->targets[i];
+  return ws->targets.size();
+}
+
+int32_t rsgpu_reconstruct_with_ws(const rsgpu_codec *h, rsgpu_reconstruct_ws *ws, uint8_t *const *shards,
+                                  const size_t *lens, const uint8_t *present, size_t n, int32_t mem, void *stream) {
+  if (!h || !ws || !present || !lens) return RSGPU_ERR_INVALID_ARGUMENT;
+  // Reuse requires the same pattern and length (src/core/recovery_plan.rs:389-413).
+  if (n != ws->present.size()) return n < ws->present.size() ? RSGPU_ERR_TOO_FEW_SHARDS : RSGPU_ERR_TOO_MANY_SHARDS;
+  for (size_t i = 0; i < n; ++i) {
+    if (present[i] && lens[i] == 0) return RSGPU_ERR_EMPTY_SHARD;
+    if (present[i] && lens[i] != ws->shard_len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  }
+  for (size_t i = 0; i < n; ++i)
+    if ((present[i] != 0) != (ws->present[i] != 0)) return RSGPU_ERR_INVALID_SHARD_FLAGS;
+  return rsgpu_reconstruct(h, shards, lens, present, n, ws->goal, ws->required.empty() ? nullptr : ws->required.data(),
+                           ws->required.size(), mem, stream);
+}
+
+int32_t rsgpu_encode_batch(const rsgpu_codec *hc, size_t n_stripes, uint8_t *const *ptrs, size_t len, int32_t mem,
+                           void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || (!ptrs && n_stripes)) return RSGPU_ERR_INVALID_ARGUMENT;
+  if (len == 0) return RSGPU_ERR_EMPTY_SHARD;
+  int rc = check_family_len(h->c, len);
+  if (rc || n_stripes == 0) return rc;
+  if (mem == RSGPU_MEM_DEVICE) return do_encode(h->c, n_stripes, ptrs, len, S(stream));
+  return run_host(h, OP_ENCODE, n_stripes, ptrs, nullptr, len, 0, nullptr, 0, nullptr, stream);
+}
+
+int32_t rsgpu_reconstruct_batch(const rsgpu_codec *hc, size_t n_stripes, uint8_t *const *ptrs,
+                                const uint8_t *present, size_t len, int32_t goal, int32_t mem, void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || (!ptrs && n_stripes) || (!present && n_stripes)) return RSGPU_ERR_INVALID_ARGUMENT;
+  if (goal == RSGPU_GOAL_REQUIRED) return RSGPU_ERR_INVALID_SHARD_FLAGS;
+  if (len == 0) return RSGPU_ERR_EMPTY_SHARD;
+  int rc = check_family_len(h->c, len);
+  if (rc || n_stripes == 0) return rc;
+  const size_t total = h->c.k + h->c.m;
+  for (size_t s = 0; s < n_stripes; ++s) {
+    size_t np = 0;
+    for (size_t i = 0; i < total; ++i) np += present[s * total + i] ? 1 : 0;
+    if (np < h->c.k) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+  }
+  if (mem == RSGPU_MEM_DEVICE) return do_reconstruct(h->c, n_stripes, ptrs, present, len, goal, nullptr, 0, S(stream));
+  return run_host(h, OP_RECONSTRUCT, n_stripes, ptrs, present, len, goal, nullptr, 0, nullptr, stream);
+}
+
+int32_t rsgpu_verify_batch(const rsgpu_codec *hc, size_t n_stripes, const uint8_t *const *ptrs, size_t len,
+                           uint8_t *ok, int32_t mem, void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || (!ptrs && n_stripes) || (!ok && n_stripes)) return RSGPU_ERR_INVALID_ARGUMENT;
+  if (len == 0) return RSGPU_ERR_EMPTY_SHARD;
+  int rc = check_family_len(h->c, len);
+  if (rc || n_stripes == 0) return rc;
+  if (mem == RSGPU_MEM_DEVICE) return do_verify(h->c, n_stripes, ptrs, len, ok, S(stream));
+  return run_host(h, OP_VERIFY, n_stripes, const_cast<uint8_t *const *>(ptrs), nullptr, len, 0, nullptr, 0, ok,
+                  stream);
+}
+
+int32_t rsgpu_get_cache_stats(const rsgpu_codec *h, rsgpu_cache_stats *out) {
+  if (!h || !out) return RSGPU_ERR_INVALID_ARGUMENT;
+  const_cast<rsgpu_codec *>(h)->c.stats(out);
+  return RSGPU_OK;
+}
+
+uint64_t rsgpu_kernel_launch_count(void) { return rsgpu::launch_counter(); }
+
+const char *rsgpu_error_string(int32_t code) {
+  switch (code) {
+    case RSGPU_OK: return "ok";
+    case RSGPU_ERR_TOO_FEW_SHARDS: return "The number of provided shards is smaller than the one in codec";
+    case RSGPU_ERR_TOO_MANY_SHARDS: return "The number of provided shards is greater than the one in codec";
+    case RSGPU_ERR_TOO_FEW_DATA_SHARDS: return "The number of provided data shards is smaller than the one in codec";
+    case RSGPU_ERR_TOO_MANY_DATA_SHARDS: return "The number of provided data shards is greater than the one in codec";
+    case RSGPU_ERR_TOO_FEW_PARITY_SHARDS: return "The number of provided parity shards is smaller than the one in codec";
+    case RSGPU_ERR_TOO_MANY_PARITY_SHARDS: return "The number of provided parity shards is greater than the one in codec";
+    case RSGPU_ERR_TOO_FEW_BUFFER_SHARDS: return "The number of provided buffer shards is smaller than the number of parity shards in codec";
+    case RSGPU_ERR_TOO_MANY_BUFFER_SHARDS: return "The number of provided buffer shards is greater than the number of parity shards in codec";
+    case RSGPU_ERR_INCORRECT_SHARD_SIZE: return "At least one of the provided shards is not of the correct size";
+    case RSGPU_ERR_TOO_FEW_SHARDS_PRESENT: return "The number of present shards is smaller than the number of data shards required for reconstruction";
+    case RSGPU_ERR_EMPTY_SHARD: return "The first shard provided is of zero length";
+    case RSGPU_ERR_INVALID_SHARD_FLAGS: return "The number of flags does not match the total number of shards";
+    case RSGPU_ERR_INVALID_INDEX: return "The data shard index provided is greater or equal to the number of data shards in codec";
+    case RSGPU_ERR_INVALID_CUSTOM_MATRIX: return "The encoding matrix is invalid, missing, or incompatible with the reconstruction workspace";
+    case RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY: return "The selected codec family is not supported for this field or configuration";
+    case RSGPU_ERR_UNSUPPORTED_LEOPARD_PROTOTYPE: return "The selected Leopard codec family is only available as a prototype skeleton in this build";
+    case RSGPU_ERR_CUDA: return "CUDA runtime error";
+    case RSGPU_ERR_OUT_OF_MEMORY: return "device memory exhausted";
+    case RSGPU_ERR_INVALID_ARGUMENT: return "invalid argument (null pointer or undersized output)";
+    case RSGPU_ERR_DEVICE_TIMEOUT: return "a bounded device wait expired";
+    case RSGPU_ERR_NO_DEVICE: return "no CUDA device available";
+    default: return "unknown error";
+  }
+}
+
+const char *rsgpu_version(void) { return "rsgpu 0.1.0 sm_100a"; }
+
+}  // extern "C"

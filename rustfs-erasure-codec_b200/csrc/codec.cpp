@@ -1,0 +1,407 @@
+// codec.cpp -- classic codec runtime: construction, validation, recovery
+// planning, the HBM-resident decode-table cache and K1/K3 submission.
+#include "codec.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+
+namespace rsgpu {
+
+static std::atomic<uint64_t> g_launches{0};
+uint64_t launch_counter_add(uint64_t n) { return g_launches.fetch_add(n) + n; }
+uint64_t launch_counter() { return g_launches.load(); }
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return RSGPU_OK;
+  if (e == cudaErrorMemoryAllocation) return RSGPU_ERR_OUT_OF_MEMORY;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return RSGPU_ERR_NO_DEVICE;
+  return RSGPU_ERR_CUDA;
+}
+
+#define RS_CUDA(expr)                          \
+  do {                                         \
+    cudaError_t e_ = (expr);                   \
+    if (e_ != cudaSuccess) return cuda_status(e_); \
+  } while (0)
+
+// ------------------------------------------------------------------ uploads
+namespace {
+struct UploadSlot {
+  void *host = nullptr;
+  size_t cap = 0;
+  cudaEvent_t done = nullptr;
+  ~UploadSlot() {
+    if (done) cudaEventDestroy(done);
+    if (host) cudaFreeHost(host);
+  }
+};
+thread_local UploadSlot t_upload;
+
+// Copies `bytes` of host data to a fresh stream-ordered device allocation
+// through a pinned, event-guarded bounce buffer.  The device block is freed
+// stream-ordered by the caller.
+int upload(const void *src, size_t bytes, void **dev, cudaStream_t s) {
+  UploadSlot &u = t_upload;
+  if (!u.done) RS_CUDA(cudaEventCreateWithFlags(&u.done, cudaEventDisableTiming));
+  RS_CUDA(cudaEventSynchronize(u.done));  // previous upload from this thread has left the buffer
+  if (u.cap < bytes) {
+    if (u.host) cudaFreeHost(u.host);
+    u.host = nullptr;
+    size_t cap = std::max<size_t>(bytes, 1 << 20);
+    RS_CUDA(cudaHostAlloc(&u.host, cap, cudaHostAllocDefault));
+    u.cap = cap;
+  }
+  std::memcpy(u.host, src, bytes);
+  RS_CUDA(cudaMallocAsync(dev, std::max<size_t>(bytes, 16), s));
+  RS_CUDA(cudaMemcpyAsync(*dev, u.host, bytes, cudaMemcpyHostToDevice, s));
+  RS_CUDA(cudaEventRecord(u.done, s));
+  return RSGPU_OK;
+}
+}  // namespace
+
+// ------------------------------------------------------------------ table pool
+TablePool::~TablePool() {
+  for (void *p : slabs_) cudaFree(p);
+}
+
+uint32_t *TablePool::get() {
+  if (free_.empty()) {
+    void *slab = nullptr;
+    if (cudaMalloc(&slab, kSlab) != cudaSuccess) return nullptr;
+    slabs_.push_back(slab);
+    const size_t n = kSlab / block_;
+    for (size_t i = 0; i < n; ++i) free_.push_back(reinterpret_cast<uint32_t *>(static_cast<char *>(slab) + i * block_));
+  }
+  uint32_t *p = free_.back();
+  free_.pop_back();
+  return p;
+}
+
+// ------------------------------------------------------------------ setup
+Codec::~Codec() {
+  cudaDeviceSynchronize();
+  pool_.reset();
+  if (d_matrix) cudaFree(d_matrix);
+  if (d_log) cudaFree(d_log);
+  if (d_exp) cudaFree(d_exp);
+  if (d_enc_tbl) cudaFree(d_enc_tbl);
+}
+
+int Codec::init_classic(const uint8_t *custom_rows) {
+  int rc = build_encoding_matrix(k, m, opts.matrix_mode, opts.fast_one_parity != 0, custom_rows, matrix);
+  if (rc != RSGPU_OK) return rc;
+  RS_CUDA(cudaGetDevice(&device));
+  const Gf8 &f = gf8();
+  RS_CUDA(cudaMalloc(&d_matrix, matrix.size()));
+  RS_CUDA(cudaMemcpy(d_matrix, matrix.data(), matrix.size(), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMalloc(&d_log, 256));
+  RS_CUDA(cudaMemcpy(d_log, f.log, 256, cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMalloc(&d_exp, 510));
+  RS_CUDA(cudaMemcpy(d_exp, f.exp, 510, cudaMemcpyHostToDevice));
+  std::vector<uint32_t> packed(packed_table_words(m, k));
+  pack_tables(&matrix[k * k], m, k, packed.data());
+  RS_CUDA(cudaMalloc(&d_enc_tbl, packed.size() * 4));
+  RS_CUDA(cudaMemcpy(d_enc_tbl, packed.data(), packed.size() * 4, cudaMemcpyHostToDevice));
+  pool_.reset(new TablePool(std::max<size_t>(256, packed_table_words(m, k) * 4)));
+  // Distinct patterns are unbounded in number, but decode tables are small:
+  // keep up to 65536 resident unless the caller set an explicit capacity.
+  capacity_ = opts.inversion_cache_capacity ? opts.inversion_cache_capacity : 65536;
+  return RSGPU_OK;
+}
+
+// ------------------------------------------------------------------ validation
+// check_piece_count!(all) + check_slices!(multi) (src/macros.rs:142-245).
+int Codec::check_all(const size_t *lens, size_t n, size_t *shard_len) const {
+  if (n < k + m) return RSGPU_ERR_TOO_FEW_SHARDS;
+  if (n > k + m) return RSGPU_ERR_TOO_MANY_SHARDS;
+  const size_t len = lens[0];
+  if (len == 0) return RSGPU_ERR_EMPTY_SHARD;
+  for (size_t i = 0; i < n; ++i)
+    if (lens[i] != len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  *shard_len = len;
+  return RSGPU_OK;
+}
+
+// src/core/recovery_plan.rs:262-517: survivors are the first k present shards;
+// targets are the missing shards the goal asks for; an inverse is needed only
+// when a missing data shard feeds some requested output.
+int Codec::plan_classic(const uint8_t *present, int goal, const uint8_t *required, size_t n_required,
+                        ClassicPlan &p) const {
+  p = ClassicPlan{};
+  const size_t total = k + m;
+  if (goal == RSGPU_GOAL_REQUIRED && n_required != k && n_required != total)
+    return p.status = RSGPU_ERR_INVALID_SHARD_FLAGS;
+  size_t n_present = 0, missing_data = 0;
+  for (size_t i = 0; i < total; ++i) {
+    if (present[i]) {
+      ++n_present;
+      if (p.survivors.size() < k) p.survivors.push_back(uint8_t(i));
+    } else if (i < k) {
+      ++missing_data;
+    }
+  }
+  if (n_present == total) {
+    p.all_present = true;
+    return RSGPU_OK;
+  }
+  if (n_present < k) return p.status = RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+  for (size_t i = 0; i < total; ++i) {
+    if (present[i]) continue;
+    bool want = goal == RSGPU_GOAL_ALL || (goal == RSGPU_GOAL_DATA && i < k) ||
+                (goal == RSGPU_GOAL_REQUIRED && i < n_required && required[i]);
+    if (!want) continue;
+    p.targets.push_back(uint8_t(i));
+    if (i < k) ++p.n_data_targets;
+  }
+  p.needs_inverse = missing_data > 0 && !p.targets.empty();
+  return RSGPU_OK;
+}
+
+// ------------------------------------------------------------------ decode cache
+static PatternKey key_of(const ClassicPlan &p, size_t k) {
+  PatternKey key;
+  // Survivors determine the inverse; targets determine the composed rows.
+  for (uint8_t s : p.survivors) key.present[s >> 6] |= 1ull << (s & 63);
+  for (uint8_t t : p.targets) key.targets[t >> 6] |= 1ull << (t & 63);
+  (void)k;
+  return key;
+}
+
+int Codec::decode_tables(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
+                         cudaStream_t s) {
+  tbls.assign(plans.size(), nullptr);
+  std::vector<DecodeTask> tasks;
+  std::vector<size_t> task_of_plan(plans.size(), SIZE_MAX);
+  std::unordered_map<PatternKey, size_t, PatternKeyHash> pending;  // new key -> task index
+  const bool use_cache = opts.inversion_cache != 0;
+  std::vector<uint32_t *> transient;  // blocks for uncached builds
+  for (size_t i = 0; i < plans.size(); ++i) {
+    const ClassicPlan &p = *plans[i];
+    if (p.all_present || p.targets.empty()) continue;
+    PatternKey key = key_of(p, k);
+    ++stats_.requests;
+    if (use_cache) {
+      auto it = cache_.find(key);
+      if (it != cache_.end()) {
+        ++stats_.hits;
+        lru_.splice(lru_.end(), lru_, it->second.lru);
+        tbls[i] = it->second.tbl;
+        continue;
+      }
+    }
+    auto pit = pending.find(key);
+    if (pit != pending.end()) {
+      task_of_plan[i] = pit->second;
+      continue;
+    }
+    ++stats_.misses;
+    DecodeTask t;
+    std::memset(&t, 0, sizeof(t));
+    std::copy(p.survivors.begin(), p.survivors.end(), t.survivors);
+    std::copy(p.targets.begin(), p.targets.end(), t.targets);
+    t.n_out = uint32_t(p.targets.size());
+    t.needs_inverse = p.needs_inverse;
+    uint32_t *blk = pool_->get();
+    if (!blk) return RSGPU_ERR_OUT_OF_MEMORY;
+    t.tbl_out = blk;
+    task_of_plan[i] = tasks.size();
+    pending.emplace(key, tasks.size());
+    tasks.push_back(t);
+    if (use_cache) {
+      if (cache_.size() >= capacity_) {
+        // Evict the least recently used entry; its block is recycled only
+        // after a device-wide sync, so no queued kernel can still read it.
+        PatternKey victim = lru_.front();
+        lru_.pop_front();
+        auto vit = cache_.find(victim);
+        retire_.push_back(vit->second.tbl);
+        cache_.erase(vit);
+        ++stats_.evictions;
+      }
+      DecodeEntry e;
+      e.tbl = blk;
+      e.survivors = p.survivors;
+      e.targets = p.targets;
+      lru_.push_back(key);
+      e.lru = std::prev(lru_.end());
+      cache_.emplace(key, std::move(e));
+      ++stats_.inserts;
+    } else {
+      transient.push_back(blk);
+    }
+  }
+  if (!tasks.empty()) {
+    void *d_tasks = nullptr;
+    int rc = upload(tasks.data(), tasks.size() * sizeof(DecodeTask), &d_tasks, s);
+    if (rc) return rc;
+    int *d_status = nullptr;
+    RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&d_status), tasks.size() * sizeof(int), s));
+    DecodeTableArgs a;
+    a.tasks = static_cast<const DecodeTask *>(d_tasks);
+    a.matrix = d_matrix;
+    a.gf_log = d_log;
+    a.gf_exp = d_exp;
+    a.status = d_status;
+    a.k = int(k);
+    int max_out = 0;
+    for (auto &t : tasks) max_out = std::max<int>(max_out, int(t.n_out));
+    RS_CUDA(launch_decode_tables(a, int(tasks.size()), max_out, s));
+    // Vandermonde and Cauchy constructions are MDS: every k x k survivor
+    // system is invertible, so their outputs can follow without a round trip.
+    // Other matrices must report a singular system before any output is
+    // written (validate-before-write), which needs the status on the host.
+    const bool mds = opts.matrix_mode == RSGPU_MATRIX_VANDERMONDE || opts.matrix_mode == RSGPU_MATRIX_CAUCHY ||
+                     (opts.fast_one_parity && m == 1);
+    int bad = 0;
+    if (!mds) {
+      std::vector<int> st(tasks.size());
+      RS_CUDA(cudaMemcpyAsync(st.data(), d_status, st.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+      RS_CUDA(cudaStreamSynchronize(s));
+      for (int v : st) bad |= v;
+    }
+    RS_CUDA(cudaFreeAsync(d_status, s));
+    RS_CUDA(cudaFreeAsync(d_tasks, s));
+    if (bad) {
+      // Drop every entry built by this call: a singular pattern must not stay cached.
+      for (auto &kv : pending) {
+        auto it = cache_.find(kv.first);
+        if (it != cache_.end()) {
+          lru_.erase(it->second.lru);
+          retire_.push_back(it->second.tbl);
+          cache_.erase(it);
+        }
+      }
+      for (uint32_t *b : transient) retire_.push_back(b);
+      return RSGPU_ERR_INVALID_CUSTOM_MATRIX;
+    }
+  }
+  for (size_t i = 0; i < plans.size(); ++i)
+    if (task_of_plan[i] != SIZE_MAX) tbls[i] = tasks[task_of_plan[i]].tbl_out;
+  for (uint32_t *b : transient) retire_.push_back(b);
+  if (retire_.size() >= 1024) {
+    RS_CUDA(cudaDeviceSynchronize());
+    for (uint32_t *b : retire_) pool_->put(b);
+    retire_.clear();
+  }
+  return RSGPU_OK;
+}
+
+void Codec::stats(rsgpu_cache_stats *out) {
+  std::lock_guard<std::mutex> g(mu_);
+  *out = stats_;
+  out->entries = cache_.size();
+  out->retained_bytes = cache_.size() * (pool_ ? pool_->block_bytes() : 0);
+}
+
+// ------------------------------------------------------------------ K1 submission
+int Codec::run_apply(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &ptrs, size_t len, bool verify,
+                     uint32_t *flags_dev, cudaStream_t s) {
+  if (jobs.empty()) return RSGPU_OK;
+  uint64_t max_tail = 0;
+  uint32_t max_out = 0;
+  int any_vec = 0;
+  for (auto &j : jobs) {
+    bool aligned = true;
+    for (uint32_t i = 0; i < uint32_t(j.n_in) + j.n_out; ++i)
+      aligned &= (reinterpret_cast<uintptr_t>(ptrs[j.ptr_off + i]) & 15) == 0;
+    j.vec_len = aligned ? (len & ~uint64_t(15)) : 0;
+    max_tail = std::max<uint64_t>(max_tail, len - j.vec_len);
+    max_out = std::max<uint32_t>(max_out, j.n_out);
+    any_vec |= j.vec_len > 0;
+  }
+  const size_t jb = jobs.size() * sizeof(JobDesc);
+  std::vector<uint8_t> blob(jb + ptrs.size() * sizeof(void *));
+  std::memcpy(blob.data(), jobs.data(), jb);
+  std::memcpy(blob.data() + jb, ptrs.data(), ptrs.size() * sizeof(void *));
+  void *d_blob = nullptr;
+  int rc = upload(blob.data(), blob.size(), &d_blob, s);
+  if (rc) return rc;
+  ApplyArgs a;
+  a.jobs = static_cast<const JobDesc *>(d_blob);
+  a.ptrs = reinterpret_cast<const uint8_t *const *>(static_cast<char *>(d_blob) + jb);
+  a.flags = flags_dev;
+  a.len = len;
+  a.n_jobs = uint32_t(jobs.size());
+  a.max_out = max_out;
+  a.any_vec = any_vec;
+  RS_CUDA(launch_apply(a, verify, max_tail, s));
+  RS_CUDA(cudaFreeAsync(d_blob, s));
+  return RSGPU_OK;
+}
+
+int Codec::encode_dev(size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s) {
+  std::vector<JobDesc> jobs(n_stripes);
+  std::vector<const uint8_t *> ptrs(shards, shards + n_stripes * (k + m));
+  for (size_t i = 0; i < n_stripes; ++i) {
+    JobDesc &j = jobs[i];
+    std::memset(&j, 0, sizeof(j));
+    j.ptr_off = uint32_t(i * (k + m));
+    j.n_in = uint16_t(k);
+    j.n_out = uint16_t(m);
+    j.tbl = d_enc_tbl;
+  }
+  return run_apply(jobs, ptrs, len, false, nullptr, s);
+}
+
+int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok_host,
+                      cudaStream_t s) {
+  std::vector<JobDesc> jobs(n_stripes);
+  std::vector<const uint8_t *> ptrs(shards, shards + n_stripes * (k + m));
+  for (size_t i = 0; i < n_stripes; ++i) {
+    JobDesc &j = jobs[i];
+    std::memset(&j, 0, sizeof(j));
+    j.ptr_off = uint32_t(i * (k + m));
+    j.n_in = uint16_t(k);
+    j.n_out = uint16_t(m);
+    j.flag_idx = uint32_t(i);
+    j.tbl = d_enc_tbl;
+  }
+  uint32_t *flags = nullptr;
+  RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&flags), n_stripes * 4, s));
+  RS_CUDA(cudaMemsetAsync(flags, 0, n_stripes * 4, s));
+  int rc = run_apply(jobs, ptrs, len, true, flags, s);
+  if (rc) return rc;
+  std::vector<uint32_t> f(n_stripes);
+  RS_CUDA(cudaMemcpyAsync(f.data(), flags, n_stripes * 4, cudaMemcpyDeviceToHost, s));
+  RS_CUDA(cudaFreeAsync(flags, s));
+  RS_CUDA(cudaStreamSynchronize(s));
+  for (size_t i = 0; i < n_stripes; ++i) ok_host[i] = f[i] ? 0 : 1;
+  return RSGPU_OK;
+}
+
+int Codec::reconstruct_dev(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len, int goal,
+                           const uint8_t *required, size_t n_required, cudaStream_t s) {
+  const size_t total = k + m;
+  std::vector<ClassicPlan> plans(n_stripes);
+  for (size_t i = 0; i < n_stripes; ++i) {
+    int rc = plan_classic(present + i * total, goal, required, n_required, plans[i]);
+    if (rc) return rc;
+  }
+  std::lock_guard<std::mutex> g(mu_);
+  std::vector<const ClassicPlan *> pp(n_stripes);
+  for (size_t i = 0; i < n_stripes; ++i) pp[i] = &plans[i];
+  std::vector<const uint32_t *> tbls;
+  int rc = decode_tables(pp, tbls, s);
+  if (rc) return rc;
+  std::vector<JobDesc> jobs;
+  std::vector<const uint8_t *> ptrs;
+  jobs.reserve(n_stripes);
+  ptrs.reserve(n_stripes * (k + m));
+  for (size_t i = 0; i < n_stripes; ++i) {
+    const ClassicPlan &p = plans[i];
+    if (p.all_present || p.targets.empty()) continue;
+    JobDesc j;
+    std::memset(&j, 0, sizeof(j));
+    j.ptr_off = uint32_t(ptrs.size());
+    j.n_in = uint16_t(k);
+    j.n_out = uint16_t(p.targets.size());
+    j.tbl = tbls[i];
+    for (uint8_t sv : p.survivors) ptrs.push_back(shards[i * total + sv]);
+    for (uint8_t t : p.targets) ptrs.push_back(shards[i * total + t]);
+    jobs.push_back(j);
+  }
+  return run_apply(jobs, ptrs, len, false, nullptr, s);
+}
+
+}  // namespace rsgpu

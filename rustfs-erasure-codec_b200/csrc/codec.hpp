@@ -1,0 +1,132 @@
+// codec.hpp -- the host runtime behind the C ABI.
+//
+// A Codec mirrors the reference `ReedSolomon<F>` (src/core/codec.rs): it owns
+// the encoding matrix (classic) or the FFT tables (Leopard), validates every
+// call with the reference's error precedence before any launch, plans
+// reconstruction, keeps decode tables resident in HBM keyed by erasure
+// pattern, and drives the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <list>
+#include <memory>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "common.hpp"
+#include "gf_host.hpp"
+#include "kernels.hpp"
+
+namespace rsgpu {
+
+// Result of the classic recovery planner for one erasure pattern
+// (src/core/recovery_plan.rs:262-517).
+struct ClassicPlan {
+  int status = RSGPU_OK;
+  bool all_present = false;
+  bool needs_inverse = false;
+  std::vector<uint8_t> survivors;  // first k present indices
+  std::vector<uint8_t> targets;    // requested missing indices, ascending
+  size_t n_data_targets = 0;
+};
+
+// 256-bit presence / target masks identify a decode-table entry.
+struct PatternKey {
+  std::array<uint64_t, 4> present{};
+  std::array<uint64_t, 4> targets{};
+  bool operator==(const PatternKey &o) const { return present == o.present && targets == o.targets; }
+};
+struct PatternKeyHash {
+  size_t operator()(const PatternKey &k) const {
+    uint64_t h = 0x9e3779b97f4a7c15ull;
+    for (int i = 0; i < 4; ++i) {
+      h ^= k.present[i] + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+      h ^= k.targets[i] + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+    }
+    return size_t(h);
+  }
+};
+
+struct DecodeEntry {
+  uint32_t *tbl = nullptr;  // device, packed tables (block of the table pool)
+  std::vector<uint8_t> survivors;
+  std::vector<uint8_t> targets;
+  std::list<PatternKey>::iterator lru;
+};
+
+// Fixed-size device blocks for decode tables, carved from large slabs so a
+// cache miss never calls cudaMalloc.
+class TablePool {
+ public:
+  explicit TablePool(size_t block_bytes) : block_(block_bytes) {}
+  ~TablePool();
+  uint32_t *get();
+  void put(uint32_t *p) { free_.push_back(p); }
+  size_t block_bytes() const { return block_; }
+  size_t slab_bytes() const { return slabs_.size() * kSlab; }
+
+ private:
+  static constexpr size_t kSlab = 8u << 20;
+  size_t block_;
+  std::vector<void *> slabs_;
+  std::vector<uint32_t *> free_;
+};
+
+struct LeopardState;  // leopard.cu
+
+class Codec {
+ public:
+  size_t k = 0, m = 0;
+  int family = RSGPU_FAMILY_CLASSIC;
+  int field = RSGPU_FIELD_GF8;
+  rsgpu_options opts{};
+  int device = 0;
+  Mat8 matrix;             // classic GF(2^8): (k+m) x k
+  std::vector<T16> tmatrix;  // classic tower field
+  // device-resident codec constants
+  uint8_t *d_matrix = nullptr;
+  uint8_t *d_log = nullptr, *d_exp = nullptr;
+  uint32_t *d_enc_tbl = nullptr;  // parity rows packed for K1
+  std::shared_ptr<LeopardState> leo;  // created where the type is complete
+
+  ~Codec();
+  int init_classic(const uint8_t *custom_rows);
+  int init_tower();
+  int init_leopard();
+
+  // ---- validation (reference error precedence)
+  int check_all(const size_t *lens, size_t n, size_t *shard_len) const;
+  int plan_classic(const uint8_t *present, int goal, const uint8_t *required, size_t n_required,
+                   ClassicPlan &out) const;
+
+  // ---- operations; pointers are device pointers unless noted
+  int encode_dev(size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s);
+  int verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok_host,
+                 cudaStream_t s);
+  int reconstruct_dev(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
+                      int goal, const uint8_t *required, size_t n_required, cudaStream_t s);
+
+  // Decode tables for a set of plans, building missing entries on the GPU (K3).
+  int decode_tables(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
+                    cudaStream_t s);
+  void stats(rsgpu_cache_stats *out);
+
+ private:
+  std::mutex mu_;
+  std::unordered_map<PatternKey, DecodeEntry, PatternKeyHash> cache_;
+  std::list<PatternKey> lru_;
+  std::unique_ptr<TablePool> pool_;
+  std::vector<uint32_t *> retire_;  // evicted blocks awaiting a device sync
+  rsgpu_cache_stats stats_{};
+  size_t capacity_ = 0;
+  int run_apply(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &ptrs, size_t len, bool verify,
+                uint32_t *flags_dev, cudaStream_t s);
+};
+
+int cuda_status(cudaError_t e);
+
+}  // namespace rsgpu

@@ -1,0 +1,42 @@
+// kernels.hpp -- launch interfaces of the sm_100a kernels (host <-> device).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+
+namespace rsgpu {
+
+// K1 arguments (k_classic.cu).
+struct ApplyArgs {
+  const JobDesc *jobs;          // device, n_jobs
+  const uint8_t *const *ptrs;   // device pointer table
+  uint32_t *flags;              // device verify flags (may be null for writes)
+  uint64_t len;                 // bytes per shard (same for every job)
+  uint32_t n_jobs;
+  uint32_t max_out;             // largest n_out over the jobs
+  int any_vec;                  // some job has vec_len > 0
+};
+cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cudaStream_t s);
+
+// K3: one erasure pattern.  Indices fit a byte because classic codecs have at
+// most 256 shards.
+struct DecodeTask {
+  uint8_t survivors[256];  // first k present shard indices, ascending
+  uint8_t targets[256];    // requested missing indices: data first, then parity
+  uint32_t n_out;
+  uint32_t needs_inverse;  // some missing data shard feeds an output
+  uint32_t pad;
+  uint32_t *tbl_out;       // device destination of the packed tables
+};
+struct DecodeTableArgs {
+  const DecodeTask *tasks;  // device
+  const uint8_t *matrix;    // device, (k+m) x k encoding matrix
+  const uint8_t *gf_log;    // device, 256
+  const uint8_t *gf_exp;    // device, >= 255
+  int *status;              // device, per task: 0 ok, 1 singular
+  int k;
+};
+cudaError_t launch_decode_tables(const DecodeTableArgs &a, int n_tasks, int max_out, cudaStream_t s);
+
+}  // namespace rsgpu

@@ -1,0 +1,31 @@
+// leopard.hpp -- family resolution plus the Leopard FFT and tower-field
+// classic codecs (device pointers; validation already done by the caller).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace rsgpu {
+
+class Codec;
+
+// src/core/leopard.rs:191-223 (resolve_codec_family) for the byte field.
+int resolve_family(int requested, int mode, size_t total, size_t parity);
+// src/core/leopard.rs:146-156, 225-270 (validate_leopard_family).
+int validate_leopard_family(int family, size_t k, size_t m);
+
+int leopard_encode(Codec &c, size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s);
+int leopard_verify(Codec &c, size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok,
+                   cudaStream_t s);
+int leopard_reconstruct(Codec &c, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
+                        int goal, const uint8_t *required, size_t n_required, cudaStream_t s);
+
+int tower_encode(Codec &c, size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s);
+int tower_verify(Codec &c, size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok,
+                 cudaStream_t s);
+int tower_reconstruct(Codec &c, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
+                      int goal, const uint8_t *required, size_t n_required, cudaStream_t s);
+
+}  // namespace rsgpu

@@ -1,0 +1,412 @@
+"""Python mirror of the rustfs-erasure-codec ``ReedSolomon`` API over librsgpu.so.
+
+This module is a thin ctypes layer over the C ABI declared in
+``include/rsgpu.h``; every byte is computed by the sm_100a kernels inside
+librsgpu.so.  There is no CPU fallback: importing this module without the
+built library raises ``ImportError``.
+
+Shards may be NumPy ``uint8`` arrays (host memory, staged through the GPU by
+the library) or ``torch.uint8`` CUDA tensors (device memory; work is queued on
+the current torch stream).  Method names and error behaviour follow the
+reference (src/core/codec.rs, encode.rs, reconstruct.rs, verify.rs): errors
+are raised as :class:`RsError` carrying the reference ``Error`` name.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "librsgpu.so")
+
+ERROR_NAMES = {
+    1: "TooFewShards", 2: "TooManyShards", 3: "TooFewDataShards", 4: "TooManyDataShards",
+    5: "TooFewParityShards", 6: "TooManyParityShards", 7: "TooFewBufferShards", 8: "TooManyBufferShards",
+    9: "IncorrectShardSize", 10: "TooFewShardsPresent", 11: "EmptyShard", 12: "InvalidShardFlags",
+    13: "InvalidIndex", 14: "InvalidCustomMatrix", 15: "UnsupportedCodecFamily",
+    16: "UnsupportedLeopardPrototype", 100: "Cuda", 101: "OutOfMemory", 102: "InvalidArgument",
+    103: "DeviceTimeout", 104: "NoDevice",
+}
+
+MEM_HOST, MEM_DEVICE = 0, 1
+FAMILY = {"classic": 0, "leopard_gf8": 1, "leopard_gf16": 2}
+LEOPARD_MODE = {"disabled": 0, "as_needed": 1, "prefer_gf16": 2, "prefer_leopard": 3}
+MATRIX_MODE = {"vandermonde": 0, "cauchy": 1, "jerasure_like": 2, "custom": 3}
+GOAL = {"all": 0, "data": 1, "required": 2}
+
+
+class RsError(Exception):
+    """A reference ``Error`` (or a device condition) returned by the library."""
+
+    def __init__(self, code: int):
+        self.code = int(code)
+        self.name = ERROR_NAMES.get(self.code, f"Error{code}")
+        super().__init__(f"{self.name}: {_lib().rsgpu_error_string(self.code).decode()}")
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [
+        ("fast_one_parity", ctypes.c_int32),
+        ("inversion_cache", ctypes.c_int32),
+        ("inversion_cache_capacity", ctypes.c_size_t),
+        ("inversion_cache_max_bytes", ctypes.c_size_t),
+        ("codec_family", ctypes.c_int32),
+        ("leopard_mode", ctypes.c_int32),
+        ("matrix_mode", ctypes.c_int32),
+        ("max_parallel_jobs", ctypes.c_size_t),
+    ]
+
+
+class CacheStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in
+                ("requests", "hits", "misses", "inserts", "evictions", "entries", "retained_bytes")]
+
+
+_L = None
+
+P = ctypes.c_void_p
+SZ = ctypes.c_size_t
+I32 = ctypes.c_int32
+PP = ctypes.POINTER(ctypes.c_void_p)
+SZP = ctypes.POINTER(ctypes.c_size_t)
+U8P = ctypes.POINTER(ctypes.c_uint8)
+
+
+def _lib():
+    global _L
+    if _L is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"librsgpu.so not found at {LIB_PATH}; build it with `python rustfs-erasure-codec_b200/build.py`")
+        L = ctypes.CDLL(LIB_PATH)
+        sigs = {
+            "rsgpu_options_default": (None, [ctypes.POINTER(_Options)]),
+            "rsgpu_codec_new": (I32, [SZ, SZ, ctypes.POINTER(_Options), PP]),
+            "rsgpu_codec_with_custom_matrix": (I32, [SZ, SZ, U8P, ctypes.POINTER(_Options), PP]),
+            "rsgpu_codec_new_gf16": (I32, [SZ, SZ, PP]),
+            "rsgpu_codec_free": (None, [P]),
+            "rsgpu_data_shard_count": (SZ, [P]),
+            "rsgpu_parity_shard_count": (SZ, [P]),
+            "rsgpu_total_shard_count": (SZ, [P]),
+            "rsgpu_codec_family": (I32, [P]),
+            "rsgpu_encoding_matrix": (I32, [P, U8P, SZ]),
+            "rsgpu_encode": (I32, [P, PP, SZP, SZ, I32, P]),
+            "rsgpu_encode_sep": (I32, [P, PP, SZP, SZ, PP, SZP, SZ, I32, P]),
+            "rsgpu_reconstruct": (I32, [P, PP, SZP, U8P, SZ, I32, U8P, SZ, I32, P]),
+            "rsgpu_verify": (I32, [P, PP, SZP, SZ, ctypes.POINTER(I32), I32, P]),
+            "rsgpu_verify_ws_new": (I32, [P, SZ, PP]),
+            "rsgpu_verify_ws_free": (None, [P]),
+            "rsgpu_verify_with_workspace": (I32, [P, PP, SZP, SZ, P, ctypes.POINTER(I32), I32, P]),
+            "rsgpu_prepare_reconstruct_ws": (I32, [P, U8P, SZ, SZ, I32, U8P, SZ, PP]),
+            "rsgpu_reconstruct_ws_free": (None, [P]),
+            "rsgpu_reconstruct_ws_targets": (SZ, [P, SZP, SZ]),
+            "rsgpu_reconstruct_with_ws": (I32, [P, P, PP, SZP, U8P, SZ, I32, P]),
+            "rsgpu_encode_batch": (I32, [P, SZ, PP, SZ, I32, P]),
+            "rsgpu_reconstruct_batch": (I32, [P, SZ, PP, U8P, SZ, I32, I32, P]),
+            "rsgpu_verify_batch": (I32, [P, SZ, PP, SZ, U8P, I32, P]),
+            "rsgpu_get_cache_stats": (I32, [P, ctypes.POINTER(CacheStats)]),
+            "rsgpu_kernel_launch_count": (ctypes.c_uint64, []),
+            "rsgpu_error_string": (ctypes.c_char_p, [I32]),
+            "rsgpu_version": (ctypes.c_char_p, []),
+        }
+        for name, (res, args) in sigs.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _L = L
+    return _L
+
+
+def lib():
+    """The loaded librsgpu.so (raises ImportError when it is not built)."""
+    return _lib()
+
+
+def kernel_launch_count() -> int:
+    return int(_lib().rsgpu_kernel_launch_count())
+
+
+def _check(rc):
+    if rc != 0:
+        raise RsError(rc)
+
+
+# ------------------------------------------------------------------ buffers
+def _is_torch_cuda(x) -> bool:
+    t = type(x)
+    return t.__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
+def _buffer_info(shards):
+    """Return (mem, ptr array, lens array, stream, keepalive) for a shard list."""
+    devs = [s is not None and _is_torch_cuda(s) for s in shards]
+    mem = MEM_DEVICE if any(devs) else MEM_HOST
+    ptrs = (ctypes.c_void_p * len(shards))()
+    lens = (ctypes.c_size_t * len(shards))()
+    keep = []
+    for i, s in enumerate(shards):
+        if s is None:
+            ptrs[i] = None
+            lens[i] = 0
+            continue
+        if mem == MEM_DEVICE:
+            if not _is_torch_cuda(s):
+                raise TypeError("mixing host and device shards in one call")
+            assert s.is_contiguous()
+            ptrs[i] = s.data_ptr()
+            lens[i] = s.numel() * s.element_size()
+        else:
+            a = s if isinstance(s, np.ndarray) else np.frombuffer(s, np.uint8)
+            if not a.flags.c_contiguous:
+                raise TypeError("host shards must be C-contiguous")
+            ptrs[i] = a.ctypes.data
+            lens[i] = a.nbytes
+            keep.append(a)
+    stream = None
+    if mem == MEM_DEVICE:
+        import torch
+
+        stream = torch.cuda.current_stream().cuda_stream
+    return mem, ptrs, lens, stream, keep
+
+
+def _flags(v, n):
+    arr = (ctypes.c_uint8 * n)()
+    for i, b in enumerate(v):
+        arr[i] = 1 if b else 0
+    return arr
+
+
+@dataclass
+class CodecOptions:
+    """src/core/options.rs:97-146."""
+
+    fast_one_parity: bool = False
+    inversion_cache: bool = True
+    inversion_cache_capacity: int = 0
+    inversion_cache_max_bytes: int = 0
+    codec_family: str = "classic"
+    leopard_mode: str = "disabled"
+    matrix_mode: str = "vandermonde"
+    max_parallel_jobs: int = 0
+
+    def _c(self):
+        o = _Options()
+        o.fast_one_parity = int(self.fast_one_parity)
+        o.inversion_cache = int(self.inversion_cache)
+        o.inversion_cache_capacity = self.inversion_cache_capacity
+        o.inversion_cache_max_bytes = self.inversion_cache_max_bytes
+        o.codec_family = FAMILY[self.codec_family]
+        o.leopard_mode = LEOPARD_MODE[self.leopard_mode]
+        o.matrix_mode = MATRIX_MODE[self.matrix_mode]
+        o.max_parallel_jobs = self.max_parallel_jobs
+        return o
+
+
+class VerifyWorkspace:
+    """src/core/workspace.rs:16-69."""
+
+    def __init__(self, codec: "ReedSolomon", shard_len: int):
+        h = ctypes.c_void_p()
+        _check(_lib().rsgpu_verify_ws_new(codec._h, shard_len, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib().rsgpu_verify_ws_free(self._h)
+            self._h = None
+
+
+class ReconstructWorkspace:
+    """src/core/workspace.rs:70-112."""
+
+    def __init__(self, h):
+        self._h = h
+
+    def targets(self) -> List[int]:
+        n = _lib().rsgpu_reconstruct_ws_targets(self._h, None, 0)
+        out = (ctypes.c_size_t * max(1, n))()
+        _lib().rsgpu_reconstruct_ws_targets(self._h, out, n)
+        return list(out)[:n]
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib().rsgpu_reconstruct_ws_free(self._h)
+            self._h = None
+
+
+class ReedSolomon:
+    """GPU drop-in for ``galois_8::ReedSolomon`` (and, with ``field='gf16'``,
+    ``galois_16::ReedSolomon``)."""
+
+    def __init__(self, data_shards: int, parity_shards: int, options: Optional[CodecOptions] = None,
+                 *, field: str = "gf8", _custom=None):
+        h = ctypes.c_void_p()
+        L = _lib()
+        if field == "gf16":
+            _check(L.rsgpu_codec_new_gf16(data_shards, parity_shards, ctypes.byref(h)))
+        elif _custom is not None:
+            o = (options or CodecOptions())._c()
+            rows = np.ascontiguousarray(np.array(_custom, np.uint8).reshape(-1))
+            _check(L.rsgpu_codec_with_custom_matrix(data_shards, parity_shards,
+                                                    rows.ctypes.data_as(U8P), ctypes.byref(o), ctypes.byref(h)))
+        else:
+            o = (options or CodecOptions())._c()
+            _check(L.rsgpu_codec_new(data_shards, parity_shards, ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.field = field
+
+    # src/core/codec.rs:264-266
+    @classmethod
+    def new(cls, data_shards, parity_shards):
+        return cls(data_shards, parity_shards)
+
+    # src/core/codec.rs:269-349
+    @classmethod
+    def with_options(cls, data_shards, parity_shards, options: CodecOptions):
+        return cls(data_shards, parity_shards, options)
+
+    # src/core/codec.rs:546-615
+    @classmethod
+    def with_custom_matrix(cls, data_shards, parity_shards, rows, options: Optional[CodecOptions] = None):
+        return cls(data_shards, parity_shards, options, _custom=rows)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib().rsgpu_codec_free(self._h)
+            self._h = None
+
+    def data_shard_count(self) -> int:
+        return _lib().rsgpu_data_shard_count(self._h)
+
+    def parity_shard_count(self) -> int:
+        return _lib().rsgpu_parity_shard_count(self._h)
+
+    def total_shard_count(self) -> int:
+        return _lib().rsgpu_total_shard_count(self._h)
+
+    def codec_family(self) -> str:
+        return {0: "classic", 1: "leopard_gf8", 2: "leopard_gf16"}[_lib().rsgpu_codec_family(self._h)]
+
+    def encoding_matrix(self) -> np.ndarray:
+        k, t = self.data_shard_count(), self.total_shard_count()
+        es = 2 if self.field == "gf16" else 1
+        out = np.zeros(t * k * es, np.uint8)
+        _check(_lib().rsgpu_encoding_matrix(self._h, out.ctypes.data_as(U8P), out.size))
+        return out.reshape((t, k, 2) if es == 2 else (t, k))
+
+    def cache_stats(self) -> CacheStats:
+        st = CacheStats()
+        _check(_lib().rsgpu_get_cache_stats(self._h, ctypes.byref(st)))
+        return st
+
+    # ---------------------------------------------------------- encode
+    def encode(self, shards: Sequence) -> None:
+        """src/core/encode.rs:935-947."""
+        mem, ptrs, lens, stream, keep = _buffer_info(list(shards))
+        _check(_lib().rsgpu_encode(self._h, ptrs, lens, len(shards), mem, stream))
+
+    def encode_sep(self, data: Sequence, parity: Sequence) -> None:
+        """src/core/encode.rs:950-972."""
+        mem, dp, dl, stream, k1 = _buffer_info(list(data))
+        mem2, pp, pl, _, k2 = _buffer_info(list(parity))
+        _check(_lib().rsgpu_encode_sep(self._h, dp, dl, len(data), pp, pl, len(parity), mem, stream))
+
+    # ---------------------------------------------------------- verify
+    def verify(self, shards: Sequence) -> bool:
+        """src/core/verify.rs:72-94."""
+        mem, ptrs, lens, stream, keep = _buffer_info(list(shards))
+        ok = ctypes.c_int32(0)
+        _check(_lib().rsgpu_verify(self._h, ptrs, lens, len(shards), ctypes.byref(ok), mem, stream))
+        return bool(ok.value)
+
+    def verify_with_workspace(self, shards: Sequence, ws: VerifyWorkspace) -> bool:
+        """src/core/verify.rs:96-115."""
+        mem, ptrs, lens, stream, keep = _buffer_info(list(shards))
+        ok = ctypes.c_int32(0)
+        _check(_lib().rsgpu_verify_with_workspace(self._h, ptrs, lens, len(shards), ws._h, ctypes.byref(ok), mem,
+                                                  stream))
+        return bool(ok.value)
+
+    # ---------------------------------------------------------- reconstruct
+    def _reconstruct(self, shards: List, goal: str, required=None):
+        # Option<Vec<u8>> semantics: None entries are missing; they receive a
+        # freshly allocated buffer when they are recovery targets.
+        present = [s is not None for s in shards]
+        filled = list(shards)
+        known = [s for s in shards if s is not None]
+        if len(shards) == self.total_shard_count() and known and sum(present) < len(shards):
+            proto = known[0]
+            n = self.data_shard_count()
+            for i, s in enumerate(shards):
+                if s is not None:
+                    continue
+                target = goal == "all" or (goal == "data" and i < n) or (
+                    goal == "required" and required is not None and i < len(required) and required[i])
+                if not target:
+                    continue
+                if _is_torch_cuda(proto):
+                    import torch
+
+                    filled[i] = torch.empty_like(proto)
+                else:
+                    filled[i] = np.zeros_like(proto)
+        mem, ptrs, lens, stream, keep = _buffer_info(filled)
+        pres = _flags(present, len(shards))
+        req = _flags(required or [], max(1, len(required or [])))
+        _check(_lib().rsgpu_reconstruct(self._h, ptrs, lens, pres, len(shards), GOAL[goal], req,
+                                        len(required or []), mem, stream))
+        for i in range(len(shards)):
+            shards[i] = filled[i]
+
+    def reconstruct(self, shards: List) -> None:
+        """src/core/reconstruct.rs:731-739: fills every missing entry (None) in place."""
+        self._reconstruct(shards, "all")
+
+    def reconstruct_data(self, shards: List) -> None:
+        """src/core/reconstruct.rs:742-750."""
+        self._reconstruct(shards, "data")
+
+    def reconstruct_some(self, shards: List, required: Sequence[bool]) -> None:
+        """src/core/reconstruct.rs:753-790."""
+        self._reconstruct(shards, "required", list(required))
+
+    def prepare_reconstruct_workspace(self, present: Sequence[bool], shard_len: int, goal: str = "all",
+                                      required=None) -> ReconstructWorkspace:
+        """src/core/reconstruct.rs:539-630."""
+        h = ctypes.c_void_p()
+        req = list(required or [])
+        _check(_lib().rsgpu_prepare_reconstruct_ws(self._h, _flags(present, len(present)), len(present), shard_len,
+                                                   GOAL[goal], _flags(req, max(1, len(req))), len(req),
+                                                   ctypes.byref(h)))
+        return ReconstructWorkspace(h)
+
+    def reconstruct_with_workspace(self, shards: List, present: Sequence[bool], ws: ReconstructWorkspace) -> None:
+        """src/core/reconstruct.rs:631-667: shards must all be buffers; missing ones are outputs."""
+        mem, ptrs, lens, stream, keep = _buffer_info(list(shards))
+        _check(_lib().rsgpu_reconstruct_with_ws(self._h, ws._h, ptrs, lens, _flags(present, len(present)),
+                                                len(shards), mem, stream))
+
+    # ---------------------------------------------------------- batched
+    def encode_batch(self, stripes: Sequence[Sequence]) -> None:
+        flat = [s for st in stripes for s in st]
+        mem, ptrs, lens, stream, keep = _buffer_info(flat)
+        _check(_lib().rsgpu_encode_batch(self._h, len(stripes), ptrs, lens[0] if flat else 0, mem, stream))
+
+    def reconstruct_batch(self, stripes: Sequence[Sequence], present: Sequence[Sequence[bool]], goal="all") -> None:
+        flat = [s for st in stripes for s in st]
+        mem, ptrs, lens, stream, keep = _buffer_info(flat)
+        pres = _flags([p for row in present for p in row], len(flat))
+        _check(_lib().rsgpu_reconstruct_batch(self._h, len(stripes), ptrs, pres, lens[0] if flat else 0,
+                                              GOAL[goal], mem, stream))
+
+    def verify_batch(self, stripes: Sequence[Sequence]) -> List[bool]:
+        flat = [s for st in stripes for s in st]
+        mem, ptrs, lens, stream, keep = _buffer_info(flat)
+        ok = (ctypes.c_uint8 * max(1, len(stripes)))()
+        _check(_lib().rsgpu_verify_batch(self._h, len(stripes), ptrs, lens[0] if flat else 0, ok, mem, stream))
+        return [bool(v) for v in list(ok)[: len(stripes)]]
