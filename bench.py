@@ -1,0 +1,456 @@
+"""Benchmark: batched classic encode + rebuild + verify on one B200 per rank.
+
+Workload (the reference's config quoted for the headline metric): classic
+galois_8 10+4 and 16+4, 1 MiB shards, 4096 stripes each, uniform-random u8
+data from a seed; every stripe gets a seeded erasure pattern of 1..m shards
+among k+m (data and parity mixed).  One step = encode, reconstruct and
+verify_with_workspace over all stripes of both geometries.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Metric: GB/s of algorithmic bytes (encode (k+m)S, reconstruct (k+e)S, verify
+(k+m)S), the same accounting as the roofline.  Inputs (137 GiB) are far
+larger than L2, so no flush is needed between steps.  Under torchrun each rank
+runs the same per-GPU workload (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rustfs-erasure-codec_b200"))
+
+SEED = 0x00EC5EED20260524  # the reference benches' BASE_SEED (benches/common/mod.rs:10)
+GEOMS = [(10, 4), (16, 4)]
+SHARD = 1 << 20
+STRIPES = 4096
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+PROFILE_FILE = os.path.join(ROOT, "profiles", "k_apply_vec_encode_10x4.txt")
+
+
+def erasure_patterns(k, m, n, seed):
+    """Seeded per-stripe erasure sets of 1..m shards among k+m."""
+    rng = np.random.default_rng(seed)
+    pats = np.ones((n, k + m), np.uint8)
+    counts = rng.integers(1, m + 1, size=n)
+    for s in range(n):
+        lost = rng.choice(k + m, size=int(counts[s]), replace=False)
+        pats[s, lost] = 0
+    return pats
+
+
+def step_bytes(k, m, pats, size):
+    n = pats.shape[0]
+    e = (k + m) - pats.sum(axis=1)
+    return int(n * (k + m) * size), int(((k + e) * size).sum()), int(n * (k + m) * size)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        import tempfile
+
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic_ratio():
+    """DRAM bytes per algorithmic byte of the encode kernel, from the committed
+    ncu summary (None when absent)."""
+    try:
+        for line in open(PROFILE_FILE):
+            if line.startswith("dram_bytes_per_algorithmic_byte:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# --------------------------------------------------------------------- CPU side
+def cpu_sample(threads):
+    """Time the oracle's threaded GFNI/AVX2 restatement of the reference's
+    fastest x86 classic path on a bounded sample: 64 stripes per geometry,
+    encode + rebuild (the same row kernel applied to recovery rows) + verify."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    n = 64
+    total_bytes = 0
+    t_total = 0.0
+    for gi, (k, m) in enumerate(GEOMS):
+        rng = np.random.default_rng(SEED + gi)
+        rc, mat = O.build_matrix(k, m)
+        block = rng.integers(0, 256, 64 * SHARD, dtype=np.uint8)
+        shards = [np.roll(block[(i % 64) * SHARD:(i % 64 + 1) * SHARD], i // 64) for i in range(n * k)]
+        flat = []
+        for s in range(n):
+            flat += shards[s * k:(s + 1) * k] + [np.zeros(SHARD, np.uint8) for _ in range(m)]
+        pats = erasure_patterns(k, m, n, SEED + 100 + gi)
+        eb, rb, vb = step_bytes(k, m, pats, SHARD)
+        t0 = time.perf_counter()
+        O.fast_encode_batch(mat, flat, n, SHARD, threads)
+        t_enc = time.perf_counter() - t0
+        # rebuild: one row-kernel call per stripe over its composed recovery rows
+        t0 = time.perf_counter()
+        for s in range(n):
+            rc, surv, targ, rows = O.classic_recovery_rows(mat, pats[s])
+            e = len(targ)
+            sub = np.zeros((k + e, k), np.uint8)
+            sub[:k] = np.eye(k, dtype=np.uint8)
+            sub[k:] = rows
+            ptrs = [flat[s * (k + m) + i] for i in surv] + [np.empty(SHARD, np.uint8) for _ in range(e)]
+            O.fast_encode_batch(sub, ptrs, 1, SHARD, threads)
+        t_rec = time.perf_counter() - t0
+        scratch = [np.empty(SHARD, np.uint8) for _ in range(n * (k + m))]
+        t0 = time.perf_counter()
+        for s in range(n):
+            for i in range(k):
+                scratch[s * (k + m) + i] = flat[s * (k + m) + i]
+        O.fast_encode_batch(mat, scratch, n, SHARD, threads)
+        ok = all(np.array_equal(scratch[s * (k + m) + k + r], flat[s * (k + m) + k + r])
+                 for s in range(n) for r in range(m))
+        t_ver = time.perf_counter() - t0
+        assert ok
+        total_bytes += eb + rb + vb
+        t_total += t_enc + t_rec + t_ver
+    return total_bytes / t_total / 1e9, O.fast_kernel_name(), n
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path (restated: no Rust toolchain
+    on this image) on the host cores, on a bounded sample of the workload."""
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sample(threads)
+    for _ in range(args.steps):
+        v, kern, n = cpu_sample(threads)
+        vals.append(v)
+    value = float(np.median(vals))
+    line = {
+        "impl": "reference", "metric": "batched classic encode+rebuild+verify GB/s (algorithmic bytes)",
+        "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "classic galois_8 10+4 and 16+4, 1 MiB shards, seeded erasures 1..m",
+                   "stripes_per_geometry_per_step": n, "flush": "inputs larger than L2"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} stripes per geometry per step, {kern} rows kernel (oracle restatement)"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------- GPU side
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--stripes", type=int, default=STRIPES)
+    ap.add_argument("--e2e-stripes", type=int, default=256)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+
+    import rsgpu
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    stream = torch.cuda.current_stream()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(SEED + rank)
+    work = []  # per geometry: dict
+    for gi, (k, m) in enumerate(GEOMS):
+        n = args.stripes
+        buf = torch.empty((n, k + m, SHARD), dtype=torch.uint8, device="cuda")
+        buf[:, :k].random_(0, 256, generator=gen)
+        codec = rsgpu.ReedSolomon(k, m)
+        offs = np.arange(n * (k + m), dtype=np.uint64) * np.uint64(SHARD)
+        ptrs = rsgpu.device_pointer_table(buf.data_ptr(), offs)
+        pats = erasure_patterns(k, m, n, SEED + 100 + gi + 1000 * rank)
+        enc = codec.prepare_batch("encode", ptrs, SHARD)
+        enc.launch()
+        torch.cuda.synchronize()
+        # Erase, then prepare (plans + device decode tables) and rebuild once.
+        ref_sum = buf.view(torch.int64).sum(dim=(1, 2))
+        lost = torch.from_numpy(pats == 0).cuda()
+        buf.masked_fill_(lost.unsqueeze(-1), 0)
+        rec = codec.prepare_batch("reconstruct", ptrs, SHARD, present=pats)
+        ver = codec.prepare_batch("verify", ptrs, SHARD)
+        rec.launch()
+        ver.launch()
+        torch.cuda.synchronize()
+        assert torch.equal(buf.view(torch.int64).sum(dim=(1, 2)), ref_sum), "rebuild changed bytes"
+        assert ver.verify_result().all(), "verify failed after rebuild"
+        eb, rb, vb = step_bytes(k, m, pats, SHARD)
+        work.append(dict(k=k, m=m, n=n, buf=buf, codec=codec, enc=enc, rec=rec, ver=ver, pats=pats, ptrs=ptrs,
+                         bytes=(eb, rb, vb)))
+    total_bytes = sum(sum(w["bytes"]) for w in work)
+
+    def step():
+        for w in work:
+            w["enc"].launch()
+            w["rec"].launch()
+            w["ver"].launch()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    launches0 = rsgpu.kernel_launch_count()
+    kern_per_step = sum(w[x].kernel_count() for w in work for x in ("enc", "rec", "ver"))
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        st.record(stream)
+        for _ in range(args.steps):
+            step()
+        en.record(stream)
+        barrier()
+    ms = st.elapsed_time(en) / args.steps
+    for w in work:
+        assert w["ver"].verify_result().all()
+    gpu_launches = kern_per_step * args.steps
+    assert rsgpu.kernel_launch_count() - launches0 == gpu_launches
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = total_bytes * world / (ms_max / 1e3) / 1e9
+
+    # Dominant kernel (10+4 encode) timed alone with events on its stream.
+    w0 = work[0]
+    enc_ms = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        w0["enc"].launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        enc_ms.append(e0.elapsed_time(e1))
+    enc_t = float(np.mean(enc_ms)) / 1e3
+    enc_bytes = w0["bytes"][0]
+    peak, peak_kind = measured_hbm_peak()
+    achieved = enc_bytes / enc_t / 1e9
+    ratio = profiled_traffic_ratio()
+
+    # Per-stripe kernel comparison (the reference's one-stripe-per-call shape)
+    # on the first 512 stripes of each geometry: one launch per stripe and op.
+    per = []
+    n_ps = min(512, args.stripes)
+    for w in work:
+        k, m = w["k"], w["m"]
+        sb = []
+        for s in range(n_ps):
+            p = w["ptrs"][s * (k + m):(s + 1) * (k + m)]
+            sb.append((w["codec"].prepare_batch("encode", p, SHARD),
+                       w["codec"].prepare_batch("reconstruct", p, SHARD, present=w["pats"][s:s + 1]),
+                       w["codec"].prepare_batch("verify", p, SHARD)))
+        per.append(sb)
+    ps_bytes = 0
+    for w in work:
+        eb, rb, vb = step_bytes(w["k"], w["m"], w["pats"][:n_ps], SHARD)
+        ps_bytes += eb + rb + vb
+
+    def per_stripe_step():
+        for sb in per:
+            for e, r, v in sb:
+                e.launch()
+                r.launch()
+                v.launch()
+
+    per_stripe_step()
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    per_stripe_step()
+    p1.record(stream)
+    torch.cuda.synchronize()
+    ps_value = ps_bytes / (p0.elapsed_time(p1) / 1e3) / 1e9
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sub_batches = []
+    for w in work:
+        k, m = w["k"], w["m"]
+        p = w["ptrs"][: n_ps * (k + m)]
+        sub_batches.append((w["codec"].prepare_batch("encode", p, SHARD),
+                            w["codec"].prepare_batch("reconstruct", p, SHARD, present=w["pats"][:n_ps]),
+                            w["codec"].prepare_batch("verify", p, SHARD)))
+    for e, r, v in sub_batches:
+        e.launch(), r.launch(), v.launch()
+    torch.cuda.synchronize()
+    b0.record(stream)
+    for e, r, v in sub_batches:
+        e.launch(), r.launch(), v.launch()
+    b1.record(stream)
+    torch.cuda.synchronize()
+    batched_same = ps_bytes / (b0.elapsed_time(b1) / 1e3) / 1e9
+    del per, sub_batches
+
+    # End to end through the public API with pinned host buffers.
+    e2e = e2e_measure(torch, rsgpu, args, rank)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, kern, n = cpu_sample(threads)
+        cpu = {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": f"{n} stripes per geometry: encode+rebuild+verify with the oracle's {kern} rows kernel"}
+
+    if rank == 0:
+        line = {
+            "metric": "batched classic encode+rebuild+verify GB/s (algorithmic bytes)",
+            "value": round(value, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "classic galois_8 10+4 and 16+4, 1 MiB shards, seeded erasures 1..m",
+                       "stripes_per_geometry": args.stripes, "ops_per_step": "encode, reconstruct, verify",
+                       "bytes_per_step_per_gpu": total_bytes, "flush": "inputs (137 GiB/GPU) larger than L2",
+                       "parallelism": f"stripes x{world} (weak, no collective)"},
+            "roofline": {"bound": "hbm", "kernel": "k_apply_vec (10+4 encode, 4096 x 1 MiB)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "traffic": None if ratio is None else int(enc_bytes * ratio),
+                         "algorithmic_bytes": enc_bytes},
+            "per_stripe": {"value": round(ps_value, 1), "unit": "GB/s", "stripes_per_geometry": n_ps,
+                           "batched_same_stripes": round(batched_same, 1),
+                           "batched_speedup": round(batched_same / ps_value, 3)},
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "gpu_launches": gpu_launches,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def e2e_measure(torch, rsgpu, args, rank):
+    """Same operations through ReedSolomon.*_batch with pinned host shards: each
+    step copies inputs host->device and results (parity, rebuilt shards, verify
+    flags) device->host inside the timed region."""
+    n = args.e2e_stripes
+    stripes = []
+    h2d = d2h = 0
+    total = 0
+    for gi, (k, m) in enumerate(GEOMS):
+        codec = rsgpu.ReedSolomon(k, m)
+        host = torch.empty((n, k + m, SHARD), dtype=torch.uint8, pin_memory=True)
+        block = np.random.default_rng(SEED + 7 + gi).integers(0, 256, 64 << 20, dtype=np.uint8)
+        arr = host.numpy()
+        flat = arr[:, :k].reshape(-1)
+        for off in range(0, flat.size, block.size):
+            flat[off:off + block.size] = block[: flat.size - off]
+        lists = arr  # (stripes, k+m, S) host array
+        pats = erasure_patterns(k, m, n, SEED + 200 + gi)
+        eb, rb, vb = step_bytes(k, m, pats, SHARD)
+        total += eb + rb + vb
+        e = (k + m) - pats.sum(axis=1)
+        h2d += n * k * SHARD + int(((k + m - e) * SHARD).sum()) + n * (k + m) * SHARD
+        d2h += n * m * SHARD + int((e * SHARD).sum()) + n
+        stripes.append((codec, lists, pats, host))
+
+    def step():
+        for codec, lists, pats, host in stripes:
+            codec.encode_batch(lists)
+            codec.reconstruct_batch(lists, pats)
+            ok = codec.verify_batch(lists)
+            assert all(ok)
+
+    step()
+    steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    for codec, lists, pats, host in stripes:
+        del host
+    return {"value": round(total / dt / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "stripes_per_geometry": n, "api": "ReedSolomon.*_batch, host memory"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

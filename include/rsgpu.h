@@ -195,6 +195,27 @@ int32_t rsgpu_verify_batch(const rsgpu_codec *codec, size_t n_stripes,
                            const uint8_t *const *shard_ptrs, size_t shard_len, uint8_t *ok,
                            int32_t mem, void *stream);
 
+/* ------------------------------------------------------------ prepared batches */
+/* A prepared batch holds the plans, decode tables and job/pointer tables of
+ * one batched operation in device memory, so that running it again is a bare
+ * kernel launch: it allocates nothing and never synchronizes, and can
+ * therefore be captured in a CUDA graph.  Shard pointers must be device
+ * pointers that stay valid for the life of the batch.  No reference
+ * counterpart (the reference re-plans every call; its closest analogue is
+ * the reusable ReconstructWorkspace, src/core/workspace.rs:70-112). */
+enum { RSGPU_OP_ENCODE = 0, RSGPU_OP_RECONSTRUCT = 1, RSGPU_OP_VERIFY = 2 };
+typedef struct rsgpu_batch rsgpu_batch;
+int32_t rsgpu_batch_prepare(const rsgpu_codec *codec, int32_t op, size_t n_stripes,
+                            uint8_t *const *shard_ptrs, const uint8_t *present, size_t shard_len,
+                            int32_t goal, rsgpu_batch **out);
+/* Queue the batch on `stream` (for verify: clear flags, then compare). */
+int32_t rsgpu_batch_launch(rsgpu_batch *batch, void *stream);
+/* Verify batches only: wait for `stream`, then write n_stripes flags. */
+int32_t rsgpu_batch_verify_result(rsgpu_batch *batch, uint8_t *ok, void *stream);
+/* Kernels one launch of this batch issues. */
+uint32_t rsgpu_batch_kernel_count(const rsgpu_batch *batch);
+void rsgpu_batch_free(rsgpu_batch *batch);
+
 /* ------------------------------------------------------------ introspection */
 /* src/core/codec.rs:412-414 (reconstruction_cache_stats): device decode-table
  * cache of this codec. */

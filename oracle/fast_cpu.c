@@ -44,17 +44,18 @@ typedef struct {
   const uint8_t *matrix;
   uint8_t *const *ptrs;
   int gfni;
+  size_t chunk;  /* columns per job: work is spread over (stripe, column chunk) */
 } job_t;
 
-__attribute__((target("avx2,gfni"))) static void rows_gfni(const job_t *j, uint8_t *const *sh) {
-  size_t k = j->k, m = j->m, len = j->len;
+__attribute__((target("avx2,gfni"))) static void rows_gfni(const job_t *j, uint8_t *const *sh, size_t x0, size_t len) {
+  size_t k = j->k, m = j->m;
   for (size_t g = 0; g < m; g += 4) {
     size_t no = m - g < 4 ? m - g : 4;
     __m256i mats[4][256];
     for (size_t o = 0; o < no; o++)
       for (size_t i = 0; i < k; i++)
         mats[o][i] = _mm256_set1_epi64x((long long)gfni_matrix(j->matrix[(k + g + o) * k + i]));
-    size_t x = 0;
+    size_t x = x0;
     for (; x + 32 <= len; x += 32) {
       __m256i acc[4] = {_mm256_setzero_si256(), _mm256_setzero_si256(), _mm256_setzero_si256(),
                         _mm256_setzero_si256()};
@@ -74,8 +75,8 @@ __attribute__((target("avx2,gfni"))) static void rows_gfni(const job_t *j, uint8
   }
 }
 
-__attribute__((target("avx2"))) static void rows_nibble(const job_t *j, uint8_t *const *sh) {
-  size_t k = j->k, m = j->m, len = j->len;
+__attribute__((target("avx2"))) static void rows_nibble(const job_t *j, uint8_t *const *sh, size_t x0, size_t len) {
+  size_t k = j->k, m = j->m;
   const __m256i mask = _mm256_set1_epi8(0x0f);
   for (size_t g = 0; g < m; g += 4) {
     size_t no = m - g < 4 ? m - g : 4;
@@ -92,7 +93,7 @@ __attribute__((target("avx2"))) static void rows_nibble(const job_t *j, uint8_t 
         lo[o][i] = _mm256_broadcastsi128_si256(a);
         hi[o][i] = _mm256_broadcastsi128_si256(b);
       }
-    size_t x = 0;
+    size_t x = x0;
     for (; x + 32 <= len; x += 32) {
       __m256i acc[4] = {_mm256_setzero_si256(), _mm256_setzero_si256(), _mm256_setzero_si256(),
                         _mm256_setzero_si256()};
@@ -117,12 +118,15 @@ __attribute__((target("avx2"))) static void rows_nibble(const job_t *j, uint8_t 
 
 static void *worker(void *arg) {
   job_t *j = (job_t *)arg;
-  for (size_t s = j->first; s < j->n_stripes; s += j->next_stripe_stride) {
+  size_t per = (j->len + j->chunk - 1) / j->chunk;
+  for (size_t q = j->first; q < j->n_stripes * per; q += j->next_stripe_stride) {
+    size_t s = q / per, c = q % per;
+    size_t x0 = c * j->chunk, x1 = x0 + j->chunk < j->len ? x0 + j->chunk : j->len;
     uint8_t *const *sh = j->ptrs + s * (j->k + j->m);
     if (j->gfni)
-      rows_gfni(j, sh);
+      rows_gfni(j, sh, x0, x1);
     else
-      rows_nibble(j, sh);
+      rows_nibble(j, sh, x0, x1);
   }
   return NULL;
 }
@@ -134,7 +138,10 @@ int orc_fast_encode_batch(size_t k, size_t m, const uint8_t *matrix, uint8_t *co
   pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)threads);
   job_t *jobs = (job_t *)malloc(sizeof(job_t) * (size_t)threads);
   for (int t = 0; t < threads; t++) {
-    job_t j = {k, m, len, n_stripes, (size_t)threads, (size_t)t, matrix, shard_ptrs, gfni};
+    size_t chunk = len / (size_t)threads + 1;
+    if (n_stripes >= (size_t)threads || chunk < (64u << 10)) chunk = len > (256u << 10) ? (256u << 10) : len;
+    chunk = (chunk + 31) & ~(size_t)31;
+    job_t j = {k, m, len, n_stripes, (size_t)threads, (size_t)t, matrix, shard_ptrs, gfni, chunk};
     jobs[t] = j;
     pthread_create(&th[t], NULL, worker, &jobs[t]);
   }

@@ -5,7 +5,7 @@
  *
  * An element is the byte pair [x, c] meaning x*X + c, with X^2 = 2X + 128
  * (EXT_POLY = [1, 2, 128], src/galois_16.rs:9-11).  The codec is the generic
- * classic codec of src/core/* instantiated with this field.
+ * classic codec of src/core/ instantiated with this field.
  */
 #include <stdlib.h>
 #include <string.h>

@@ -26,6 +26,19 @@ struct rsgpu_codec {
   std::mutex io_mu;
 };
 
+struct rsgpu_batch {
+  rsgpu_codec *codec = nullptr;
+  int op = 0;
+  size_t n_stripes = 0;
+  rsgpu::ApplyLaunch apply;                // classic families
+  std::shared_ptr<rsgpu::LeoLaunch> leo;   // Leopard families
+  uint32_t *flags = nullptr;               // verify flags (device)
+  ~rsgpu_batch() {
+    apply.release(nullptr);
+    if (flags) cudaFree(flags);
+  }
+};
+
 struct rsgpu_verify_ws {
   size_t shard_len = 0;
 };
@@ -495,6 +508,75 @@ int32_t rsgpu_verify_batch(const rsgpu_codec *hc, size_t n_stripes, const uint8_
   return run_host(h, OP_VERIFY, n_stripes, const_cast<uint8_t *const *>(ptrs), nullptr, len, 0, nullptr, 0, ok,
                   stream);
 }
+
+int32_t rsgpu_batch_prepare(const rsgpu_codec *hc, int32_t op, size_t n_stripes, uint8_t *const *ptrs,
+                            const uint8_t *present, size_t len, int32_t goal, rsgpu_batch **out) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || !out || (!ptrs && n_stripes)) return RSGPU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (op < RSGPU_OP_ENCODE || op > RSGPU_OP_VERIFY) return RSGPU_ERR_INVALID_ARGUMENT;
+  if (op == RSGPU_OP_RECONSTRUCT && (!present || goal == RSGPU_GOAL_REQUIRED)) return RSGPU_ERR_INVALID_SHARD_FLAGS;
+  if (len == 0) return RSGPU_ERR_EMPTY_SHARD;
+  Codec &c = h->c;
+  int rc = check_family_len(c, len);
+  if (rc) return rc;
+  const size_t total = c.k + c.m;
+  if (op == RSGPU_OP_RECONSTRUCT)
+    for (size_t s = 0; s < n_stripes; ++s) {
+      size_t np = 0;
+      for (size_t i = 0; i < total; ++i) np += present[s * total + i] ? 1 : 0;
+      if (np < c.k) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+    }
+  std::unique_ptr<rsgpu_batch> b(new (std::nothrow) rsgpu_batch());
+  if (!b) return RSGPU_ERR_OUT_OF_MEMORY;
+  b->codec = h;
+  b->op = op;
+  b->n_stripes = n_stripes;
+  if (op == RSGPU_OP_VERIFY) {
+    RS_CUDA(cudaMalloc(reinterpret_cast<void **>(&b->flags), std::max<size_t>(n_stripes, 1) * 4));
+    RS_CUDA(cudaMemset(b->flags, 0, std::max<size_t>(n_stripes, 1) * 4));
+  }
+  if (c.family != RSGPU_FAMILY_CLASSIC || c.field != RSGPU_FIELD_GF8) {
+    rc = rsgpu::prepare_other(c, op, n_stripes, ptrs, present, len, goal, b->flags, b->leo);
+  } else {
+    std::vector<rsgpu::JobDesc> jobs;
+    std::vector<const uint8_t *> dptrs;
+    if (op == RSGPU_OP_RECONSTRUCT) {
+      rc = c.reconstruct_jobs(n_stripes, ptrs, present, goal, nullptr, 0, jobs, dptrs, nullptr);
+      if (rc == RSGPU_OK) rc = rsgpu::cuda_status(cudaDeviceSynchronize());
+    } else {
+      rc = c.encode_jobs(n_stripes, ptrs, jobs, dptrs, op == RSGPU_OP_VERIFY);
+    }
+    if (rc == RSGPU_OK) rc = b->apply.build(jobs, dptrs, len, op == RSGPU_OP_VERIFY, b->flags, nullptr, true);
+  }
+  if (rc) return rc;
+  *out = b.release();
+  return RSGPU_OK;
+}
+
+int32_t rsgpu_batch_launch(rsgpu_batch *b, void *stream) {
+  if (!b) return RSGPU_ERR_INVALID_ARGUMENT;
+  if (b->flags) RS_CUDA(cudaMemsetAsync(b->flags, 0, std::max<size_t>(b->n_stripes, 1) * 4, S(stream)));
+  if (b->leo) return rsgpu::leo_launch(*b->leo, S(stream));
+  return b->apply.launch(S(stream));
+}
+
+int32_t rsgpu_batch_verify_result(rsgpu_batch *b, uint8_t *ok, void *stream) {
+  if (!b || !ok || b->op != RSGPU_OP_VERIFY) return RSGPU_ERR_INVALID_ARGUMENT;
+  std::vector<uint32_t> f(b->n_stripes);
+  RS_CUDA(cudaMemcpyAsync(f.data(), b->flags, b->n_stripes * 4, cudaMemcpyDeviceToHost, S(stream)));
+  RS_CUDA(cudaStreamSynchronize(S(stream)));
+  for (size_t i = 0; i < b->n_stripes; ++i) ok[i] = f[i] ? 0 : 1;
+  return RSGPU_OK;
+}
+
+uint32_t rsgpu_batch_kernel_count(const rsgpu_batch *b) {
+  if (!b) return 0;
+  if (b->leo) return rsgpu::leo_kernel_count(*b->leo);
+  return uint32_t((b->apply.args.any_vec ? 1 : 0) + (b->apply.max_tail ? 1 : 0));
+}
+
+void rsgpu_batch_free(rsgpu_batch *b) { delete b; }
 
 int32_t rsgpu_get_cache_stats(const rsgpu_codec *h, rsgpu_cache_stats *out) {
   if (!h || !out) return RSGPU_ERR_INVALID_ARGUMENT;

@@ -295,10 +295,10 @@ void Codec::stats(rsgpu_cache_stats *out) {
 }
 
 // ------------------------------------------------------------------ K1 submission
-int Codec::run_apply(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &ptrs, size_t len, bool verify,
-                     uint32_t *flags_dev, cudaStream_t s) {
-  if (jobs.empty()) return RSGPU_OK;
-  uint64_t max_tail = 0;
+int ApplyLaunch::build(std::vector<JobDesc> &jobs, const std::vector<const uint8_t *> &ptrs, size_t len, bool vfy,
+                       uint32_t *flags, cudaStream_t s, bool persistent) {
+  verify = vfy;
+  max_tail = 0;
   uint32_t max_out = 0;
   int any_vec = 0;
   for (auto &j : jobs) {
@@ -314,49 +314,76 @@ int Codec::run_apply(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &p
   std::vector<uint8_t> blob(jb + ptrs.size() * sizeof(void *));
   std::memcpy(blob.data(), jobs.data(), jb);
   std::memcpy(blob.data() + jb, ptrs.data(), ptrs.size() * sizeof(void *));
-  void *d_blob = nullptr;
-  int rc = upload(blob.data(), blob.size(), &d_blob, s);
+  owned = persistent;
+  if (persistent) {
+    RS_CUDA(cudaMalloc(&d_blob, std::max<size_t>(blob.size(), 16)));
+    RS_CUDA(cudaMemcpy(d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  } else {
+    int rc = upload(blob.data(), blob.size(), &d_blob, s);
+    if (rc) return rc;
+  }
+  args.jobs = static_cast<const JobDesc *>(d_blob);
+  args.ptrs = reinterpret_cast<const uint8_t *const *>(static_cast<char *>(d_blob) + jb);
+  args.flags = flags;
+  args.len = len;
+  args.n_jobs = uint32_t(jobs.size());
+  args.max_out = max_out;
+  args.any_vec = any_vec;
+  return RSGPU_OK;
+}
+
+int ApplyLaunch::launch(cudaStream_t s) const {
+  if (args.n_jobs == 0) return RSGPU_OK;
+  return cuda_status(launch_apply(args, verify, max_tail, s));
+}
+
+void ApplyLaunch::release(cudaStream_t s) {
+  if (!d_blob) return;
+  if (owned)
+    cudaFree(d_blob);
+  else
+    cudaFreeAsync(d_blob, s);
+  d_blob = nullptr;
+}
+
+int Codec::run_apply(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &ptrs, size_t len, bool verify,
+                     uint32_t *flags_dev, cudaStream_t s) {
+  if (jobs.empty()) return RSGPU_OK;
+  ApplyLaunch l;
+  int rc = l.build(jobs, ptrs, len, verify, flags_dev, s, false);
   if (rc) return rc;
-  ApplyArgs a;
-  a.jobs = static_cast<const JobDesc *>(d_blob);
-  a.ptrs = reinterpret_cast<const uint8_t *const *>(static_cast<char *>(d_blob) + jb);
-  a.flags = flags_dev;
-  a.len = len;
-  a.n_jobs = uint32_t(jobs.size());
-  a.max_out = max_out;
-  a.any_vec = any_vec;
-  RS_CUDA(launch_apply(a, verify, max_tail, s));
-  RS_CUDA(cudaFreeAsync(d_blob, s));
+  rc = l.launch(s);
+  l.release(s);
+  return rc;
+}
+
+int Codec::encode_jobs(size_t n_stripes, uint8_t *const *shards, std::vector<JobDesc> &jobs,
+                       std::vector<const uint8_t *> &ptrs, bool verify) {
+  jobs.assign(n_stripes, JobDesc{});
+  ptrs.assign(shards, shards + n_stripes * (k + m));
+  for (size_t i = 0; i < n_stripes; ++i) {
+    JobDesc &j = jobs[i];
+    j.ptr_off = uint32_t(i * (k + m));
+    j.n_in = uint16_t(k);
+    j.n_out = uint16_t(m);
+    j.flag_idx = verify ? uint32_t(i) : 0;
+    j.tbl = d_enc_tbl;
+  }
   return RSGPU_OK;
 }
 
 int Codec::encode_dev(size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s) {
-  std::vector<JobDesc> jobs(n_stripes);
-  std::vector<const uint8_t *> ptrs(shards, shards + n_stripes * (k + m));
-  for (size_t i = 0; i < n_stripes; ++i) {
-    JobDesc &j = jobs[i];
-    std::memset(&j, 0, sizeof(j));
-    j.ptr_off = uint32_t(i * (k + m));
-    j.n_in = uint16_t(k);
-    j.n_out = uint16_t(m);
-    j.tbl = d_enc_tbl;
-  }
+  std::vector<JobDesc> jobs;
+  std::vector<const uint8_t *> ptrs;
+  encode_jobs(n_stripes, shards, jobs, ptrs, false);
   return run_apply(jobs, ptrs, len, false, nullptr, s);
 }
 
 int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok_host,
                       cudaStream_t s) {
-  std::vector<JobDesc> jobs(n_stripes);
-  std::vector<const uint8_t *> ptrs(shards, shards + n_stripes * (k + m));
-  for (size_t i = 0; i < n_stripes; ++i) {
-    JobDesc &j = jobs[i];
-    std::memset(&j, 0, sizeof(j));
-    j.ptr_off = uint32_t(i * (k + m));
-    j.n_in = uint16_t(k);
-    j.n_out = uint16_t(m);
-    j.flag_idx = uint32_t(i);
-    j.tbl = d_enc_tbl;
-  }
+  std::vector<JobDesc> jobs;
+  std::vector<const uint8_t *> ptrs;
+  encode_jobs(n_stripes, const_cast<uint8_t *const *>(shards), jobs, ptrs, true);
   uint32_t *flags = nullptr;
   RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&flags), n_stripes * 4, s));
   RS_CUDA(cudaMemsetAsync(flags, 0, n_stripes * 4, s));
@@ -370,8 +397,9 @@ int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len
   return RSGPU_OK;
 }
 
-int Codec::reconstruct_dev(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len, int goal,
-                           const uint8_t *required, size_t n_required, cudaStream_t s) {
+int Codec::reconstruct_jobs(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, int goal,
+                            const uint8_t *required, size_t n_required, std::vector<JobDesc> &jobs,
+                            std::vector<const uint8_t *> &ptrs, cudaStream_t s) {
   const size_t total = k + m;
   std::vector<ClassicPlan> plans(n_stripes);
   for (size_t i = 0; i < n_stripes; ++i) {
@@ -384,15 +412,14 @@ int Codec::reconstruct_dev(size_t n_stripes, uint8_t *const *shards, const uint8
   std::vector<const uint32_t *> tbls;
   int rc = decode_tables(pp, tbls, s);
   if (rc) return rc;
-  std::vector<JobDesc> jobs;
-  std::vector<const uint8_t *> ptrs;
+  jobs.clear();
+  ptrs.clear();
   jobs.reserve(n_stripes);
-  ptrs.reserve(n_stripes * (k + m));
+  ptrs.reserve(n_stripes * total);
   for (size_t i = 0; i < n_stripes; ++i) {
     const ClassicPlan &p = plans[i];
     if (p.all_present || p.targets.empty()) continue;
-    JobDesc j;
-    std::memset(&j, 0, sizeof(j));
+    JobDesc j{};
     j.ptr_off = uint32_t(ptrs.size());
     j.n_in = uint16_t(k);
     j.n_out = uint16_t(p.targets.size());
@@ -401,6 +428,15 @@ int Codec::reconstruct_dev(size_t n_stripes, uint8_t *const *shards, const uint8
     for (uint8_t t : p.targets) ptrs.push_back(shards[i * total + t]);
     jobs.push_back(j);
   }
+  return RSGPU_OK;
+}
+
+int Codec::reconstruct_dev(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len, int goal,
+                           const uint8_t *required, size_t n_required, cudaStream_t s) {
+  std::vector<JobDesc> jobs;
+  std::vector<const uint8_t *> ptrs;
+  int rc = reconstruct_jobs(n_stripes, shards, present, goal, required, n_required, jobs, ptrs, s);
+  if (rc) return rc;
   return run_apply(jobs, ptrs, len, false, nullptr, s);
 }
 

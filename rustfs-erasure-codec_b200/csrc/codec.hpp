@@ -78,6 +78,21 @@ class TablePool {
 
 struct LeopardState;  // leopard.cu
 
+// A K1 launch whose job and pointer tables live in device memory.  Built once
+// and launched any number of times (launch() allocates and synchronizes
+// nothing, so it can be captured in a CUDA graph).
+struct ApplyLaunch {
+  void *d_blob = nullptr;  // JobDesc[n_jobs] followed by the pointer table
+  bool owned = false;      // cudaMalloc'd (prepared batch) vs stream-ordered
+  ApplyArgs args{};
+  uint64_t max_tail = 0;
+  bool verify = false;
+  int build(std::vector<JobDesc> &jobs, const std::vector<const uint8_t *> &ptrs, size_t len, bool verify,
+            uint32_t *flags, cudaStream_t s, bool persistent);
+  int launch(cudaStream_t s) const;
+  void release(cudaStream_t s);
+};
+
 class Codec {
  public:
   size_t k = 0, m = 0;
@@ -125,6 +140,14 @@ class Codec {
   size_t capacity_ = 0;
   int run_apply(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &ptrs, size_t len, bool verify,
                 uint32_t *flags_dev, cudaStream_t s);
+
+ public:
+  // Job lists for the three classic operations over device pointers.
+  int encode_jobs(size_t n_stripes, uint8_t *const *shards, std::vector<JobDesc> &jobs,
+                  std::vector<const uint8_t *> &ptrs, bool verify);
+  int reconstruct_jobs(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, int goal,
+                       const uint8_t *required, size_t n_required, std::vector<JobDesc> &jobs,
+                       std::vector<const uint8_t *> &ptrs, cudaStream_t s);
 };
 
 int cuda_status(cudaError_t e);

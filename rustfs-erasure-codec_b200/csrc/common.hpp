@@ -30,12 +30,17 @@ struct JobDesc {
 };
 static_assert(sizeof(JobDesc) == 32, "JobDesc layout");
 
-// Packed table layout for one coefficient matrix of n_out x n_in:
-// for each group g of 4 outputs, for each input j, 32 words:
-//   word n      (n < 16): bytes r = c[4g+r][j] * n          (low nibble)
-//   word 16 + n (n < 16): bytes r = c[4g+r][j] * (n << 4)   (high nibble)
+// Packed table layout for one coefficient matrix of n_out x n_in: for each
+// group g of 4 outputs and each input j, kTableWords words (byte r of a word
+// belongs to output 4g+r):
+//   [0, 16)   c * n          n = 0..15   (4+4 split: low nibble)
+//   [16, 32)  c * (n << 4)   n = 0..15   (4+4 split: high nibble)
+//   [32, 64)  c * i          i = 0..31   (5+3 split: low five bits)
+//   [64, 72)  for output r: words 64+2r, 65+2r hold the bytes c_r * (h << 5),
+//             h = 0..7        (5+3 split: high three bits, one byte per h)
+constexpr int kTableWords = 72;
 inline size_t packed_table_words(size_t n_out, size_t n_in) {
-  return ((n_out + 3) / 4) * n_in * 32;
+  return ((n_out + 3) / 4) * n_in * kTableWords;
 }
 
 uint64_t launch_counter_add(uint64_t n);

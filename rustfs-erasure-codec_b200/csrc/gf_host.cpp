@@ -3,6 +3,7 @@
 
 #include <cstring>
 
+#include "common.hpp"
 #include "rsgpu.h"
 
 namespace rsgpu {
@@ -263,18 +264,18 @@ void pack_tables(const uint8_t *rows, size_t n_out, size_t n_in, uint32_t *out) 
   const size_t groups = (n_out + 3) / 4;
   for (size_t g = 0; g < groups; ++g)
     for (size_t j = 0; j < n_in; ++j) {
-      uint32_t *t = out + (g * n_in + j) * 32;
-      for (unsigned n = 0; n < 16; ++n) {
-        uint32_t lo = 0, hi = 0;
-        for (unsigned r = 0; r < 4; ++r) {
-          size_t o = g * 4 + r;
-          if (o >= n_out) break;
-          uint8_t c = rows[o * n_in + j];
-          lo |= uint32_t(f.mul[c][n]) << (8 * r);
-          hi |= uint32_t(f.mul[c][n << 4]) << (8 * r);
+      uint32_t *t = out + (g * n_in + j) * kTableWords;
+      for (unsigned i = 0; i < unsigned(kTableWords); ++i) t[i] = 0;
+      for (unsigned r = 0; r < 4; ++r) {
+        const size_t o = g * 4 + r;
+        if (o >= n_out) break;
+        const uint8_t c = rows[o * n_in + j];
+        for (unsigned n = 0; n < 16; ++n) {
+          t[n] |= uint32_t(f.mul[c][n]) << (8 * r);
+          t[16 + n] |= uint32_t(f.mul[c][n << 4]) << (8 * r);
         }
-        t[n] = lo;
-        t[16 + n] = hi;
+        for (unsigned i = 0; i < 32; ++i) t[32 + i] |= uint32_t(f.mul[c][i]) << (8 * r);
+        for (unsigned h = 0; h < 8; ++h) t[64 + 2 * r + (h >> 2)] |= uint32_t(f.mul[c][h << 5]) << (8 * (h & 3));
       }
     }
 }

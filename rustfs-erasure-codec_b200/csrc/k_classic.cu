@@ -4,22 +4,28 @@
 //   for encode, reconstruct (composed recovery rows) and verify (compare
 //   instead of store).  It replaces the reference's row dot-product loops
 //   (src/core/encode.rs:532-602, src/galois_8/x86/gfni_rows.rs:15-288).
-//   Design: each thread owns 16 byte columns of one stripe and reads every
-//   input shard exactly once with a coalesced 128-bit load.  A product
-//   c * x is the XOR of two 16-entry nibble-table lookups; the tables of four
-//   outputs are packed into one 32-bit word per entry, so one lookup serves
-//   four parity rows at once.  The lookups are warp shuffles: lane l holds
-//   table entry (l & 15), so a shuffle indexed by the raw shifted data word
-//   (only bits 0..3 matter once the 16-entry table is mirrored into lanes
-//   16..31) performs 32 independent table lookups without touching shared
-//   memory and without bank conflicts.  All m outputs of a column are
-//   accumulated in registers and written once.
+//   Design: each thread owns 16 (or 32) byte columns of one stripe and reads
+//   every input shard exactly once with coalesced 128-bit loads.  Products
+//   are table lookups split over the bits of the data byte, and the tables of
+//   four outputs are packed into one 32-bit word per entry, so one lookup
+//   serves four parity rows.  Two formulations share the work so that
+//   neither the shuffle (LSU) pipe nor the integer (ALU) pipe saturates:
+//     4+4 split: two warp-shuffle lookups into 16-entry tables held one entry
+//       per lane (mirrored into lanes 16..31, so the raw shifted data word is
+//       a valid index: the shuffle only reads bits 0..4);
+//     5+3 split: one shuffle into a 32-entry table for the low five bits and
+//       one byte-permute (PRMT) per output for the high three bits, whose
+//       eight-entry byte table fits the two PRMT source registers and whose
+//       result lands directly in per-output column order.
+//   All m outputs of a column are accumulated in registers and written once.
 //
 // K3 (decode tables): Gauss-Jordan inversion of the selected survivor rows,
 //   composition of the requested parity rows and packing of the nibble
 //   tables, one CTA per erasure pattern (src/core/reconstruct.rs:1068-1174,
 //   src/core/recovery_plan.rs:425-517).
 #include <cuda_runtime.h>
+
+#include <cstdlib>
 
 #include "common.hpp"
 #include "kernels.hpp"
@@ -54,6 +60,21 @@ __device__ __forceinline__ void transpose4(const uint32_t *a, uint32_t *o) {
   o[3] = __byte_perm(t2, t3, 0x7632);
 }
 
+// 5+3 split, shuffle half: low five bits of each byte of w index t5.
+__device__ __forceinline__ void mac4_lo5(uint32_t w, uint32_t t5, uint32_t *a) {
+  a[0] ^= tshfl(t5, w);
+  a[1] ^= tshfl(t5, w >> 8);
+  a[2] ^= tshfl(t5, w >> 16);
+  a[3] ^= tshfl(t5, w >> 24);
+}
+
+// 5+3 split, PRMT half: selector nibble c = high three bits of byte c of w.
+__device__ __forceinline__ uint32_t hi3_selector(uint32_t w) {
+  const uint32_t x = (w >> 5) & 0x07070707u;
+  const uint32_t y = x | ((w >> 9) & 0x00707070u);
+  return __byte_perm(y, 0, 0x3320);
+}
+
 __device__ __forceinline__ uint4 ld_stream(const uint8_t *p) {
   uint4 v;
   asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
@@ -68,71 +89,113 @@ __device__ __forceinline__ void st_stream(uint8_t *p, uint4 v) {
                : "memory");
 }
 
-constexpr int kBatch = 8;  // input vectors kept in flight per thread
 
-// NG = number of 4-output groups handled in one pass (outputs g*4 .. g*4+3).
-template <int NG, bool VERIFY>
+// One tile = kApplyThreads threads x V 128-bit vectors of columns of one job.
+// NG = number of 4-output groups per pass (outputs g*4 .. g*4+3).
+// MIX: 0 = every input uses the 4+4 split, 1 = odd inputs use 5+3, 2 = all 5+3.
+template <int NG, int V, int kBatch, int MIX, bool VERIFY>
 __global__ void __launch_bounds__(kApplyThreads) k_apply_vec(ApplyArgs a) {
+  constexpr uint32_t kTile = kApplyThreads * kApplyVec * V;
   const uint32_t lane = threadIdx.x & 31;
-  const uint64_t tiles_per_job = (a.len + kApplyTile - 1) / kApplyTile;
-  const uint64_t total = tiles_per_job * a.n_jobs;
-  for (uint64_t t = blockIdx.x; t < total; t += gridDim.x) {
-    const uint32_t job = uint32_t(t / tiles_per_job);
-    const uint64_t col = (t - uint64_t(job) * tiles_per_job) * kApplyTile + uint64_t(threadIdx.x) * kApplyVec;
+  const uint32_t tiles_per_job = uint32_t((a.len + kTile - 1) / kTile);
+  const uint32_t total = tiles_per_job * a.n_jobs;
+  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+    const uint32_t job = t / tiles_per_job;
+    const uint64_t tile_base = uint64_t(t - job * tiles_per_job) * kTile;
     const JobDesc d = a.jobs[job];
-    if ((t - uint64_t(job) * tiles_per_job) * kApplyTile >= d.vec_len) continue;  // CTA-uniform
-    const bool active = col < d.vec_len;
+    if (tile_base >= d.vec_len) continue;  // CTA-uniform
+    // Thread column of vector v: tile_base + (v * kApplyThreads + tid) * 16, so a
+    // warp's 32 loads of one vector cover 512 contiguous bytes.
+    uint64_t col[V];
+    bool active[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      col[v] = tile_base + (uint64_t(v) * kApplyThreads + threadIdx.x) * kApplyVec;
+      active[v] = col[v] < d.vec_len;
+    }
     const uint8_t *const *ptr = a.ptrs + d.ptr_off;
     const uint32_t n_in = d.n_in;
     for (uint32_t g0 = 0; g0 * 4 < d.n_out; g0 += NG) {
-      uint32_t acc[NG][16];
+      uint32_t acc[NG][V][16];   // per column: 4 packed outputs
+      uint32_t oacc[NG][V][16];  // per output r, word w (index r*4+w): 4 columns
 #pragma unroll
       for (int g = 0; g < NG; ++g)
 #pragma unroll
-        for (int i = 0; i < 16; ++i) acc[g][i] = 0;
+        for (int v = 0; v < V; ++v)
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[g][v][i] = oacc[g][v][i] = 0;
       for (uint32_t j0 = 0; j0 < n_in; j0 += kBatch) {
-        uint4 v[kBatch];
+        uint4 x[kBatch][V];
 #pragma unroll
         for (int b = 0; b < kBatch; ++b) {
-          v[b] = make_uint4(0, 0, 0, 0);
-          if (active && j0 + b < n_in) v[b] = ld_stream(ptr[j0 + b] + col);
+          const uint8_t *src = (j0 + b < n_in) ? ptr[j0 + b] : nullptr;
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            x[b][v] = make_uint4(0, 0, 0, 0);
+            if (src && active[v]) x[b][v] = ld_stream(src + col[v]);
+          }
         }
 #pragma unroll
         for (int b = 0; b < kBatch; ++b) {
           if (j0 + b >= n_in) break;  // warp-uniform
+          const bool split53 = MIX == 2 || (MIX == 1 && (b & 1));  // compile-time
 #pragma unroll
           for (int g = 0; g < NG; ++g) {
-            const uint32_t *tb = d.tbl + ((g0 + g) * n_in + (j0 + b)) * 32;
-            const uint32_t lo = __ldg(tb + (lane & 15));
-            const uint32_t hi = __ldg(tb + 16 + (lane & 15));
-            mac4(v[b].x, lo, hi, &acc[g][0]);
-            mac4(v[b].y, lo, hi, &acc[g][4]);
-            mac4(v[b].z, lo, hi, &acc[g][8]);
-            mac4(v[b].w, lo, hi, &acc[g][12]);
+            const uint32_t *tb = d.tbl + ((g0 + g) * n_in + (j0 + b)) * kTableWords;
+            if (!split53) {
+              const uint32_t lo = __ldg(tb + (lane & 15));
+              const uint32_t hi = __ldg(tb + 16 + (lane & 15));
+#pragma unroll
+              for (int v = 0; v < V; ++v) {
+                mac4(x[b][v].x, lo, hi, &acc[g][v][0]);
+                mac4(x[b][v].y, lo, hi, &acc[g][v][4]);
+                mac4(x[b][v].z, lo, hi, &acc[g][v][8]);
+                mac4(x[b][v].w, lo, hi, &acc[g][v][12]);
+              }
+            } else {
+              const uint32_t t5 = __ldg(tb + 32 + lane);
+              const uint4 h01 = __ldg(reinterpret_cast<const uint4 *>(tb + 64));
+              const uint4 h23 = __ldg(reinterpret_cast<const uint4 *>(tb + 68));
+              const uint32_t h3[8] = {h01.x, h01.y, h01.z, h01.w, h23.x, h23.y, h23.z, h23.w};
+#pragma unroll
+              for (int v = 0; v < V; ++v) {
+                const uint32_t wv[4] = {x[b][v].x, x[b][v].y, x[b][v].z, x[b][v].w};
+#pragma unroll
+                for (int w = 0; w < 4; ++w) {
+                  mac4_lo5(wv[w], t5, &acc[g][v][w * 4]);
+                  const uint32_t sel = hi3_selector(wv[w]);
+#pragma unroll
+                  for (int r = 0; r < 4; ++r) oacc[g][v][r * 4 + w] ^= __byte_perm(h3[2 * r], h3[2 * r + 1], sel);
+                }
+              }
+            }
           }
         }
       }
       bool bad = false;
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
-        uint32_t o[4][4];  // [output r][word w]
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
-          uint32_t tmp[4];
-          transpose4(&acc[g][w * 4], tmp);
+        for (int v = 0; v < V; ++v) {
+          uint32_t o[4][4];  // [output r][word w]
 #pragma unroll
-          for (int r = 0; r < 4; ++r) o[r][w] = tmp[r];
-        }
+          for (int w = 0; w < 4; ++w) {
+            uint32_t tmp[4];
+            transpose4(&acc[g][v][w * 4], tmp);
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const uint32_t out = (g0 + g) * 4 + r;
-          if (out < d.n_out && active) {
-            uint8_t *dst = const_cast<uint8_t *>(ptr[n_in + out]) + col;
-            if (VERIFY) {
-              uint4 e = ld_stream(dst);
-              bad |= (e.x != o[r][0]) | (e.y != o[r][1]) | (e.z != o[r][2]) | (e.w != o[r][3]);
-            } else {
-              st_stream(dst, make_uint4(o[r][0], o[r][1], o[r][2], o[r][3]));
+            for (int r = 0; r < 4; ++r) o[r][w] = tmp[r] ^ (MIX ? oacc[g][v][r * 4 + w] : 0u);
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const uint32_t out = (g0 + g) * 4 + r;
+            if (out < d.n_out && active[v]) {
+              uint8_t *dst = const_cast<uint8_t *>(ptr[n_in + out]) + col[v];
+              if (VERIFY) {
+                uint4 e = ld_stream(dst);
+                bad |= (e.x != o[r][0]) | (e.y != o[r][1]) | (e.z != o[r][2]) | (e.w != o[r][3]);
+              } else {
+                st_stream(dst, make_uint4(o[r][0], o[r][1], o[r][2], o[r][3]));
+              }
             }
           }
         }
@@ -162,7 +225,7 @@ __global__ void k_apply_tail(ApplyArgs a, uint64_t max_tail) {
       uint32_t acc = 0;
       for (uint32_t j = 0; j < d.n_in; ++j) {
         const uint32_t x = ptr[j][col];
-        const uint32_t *tb = d.tbl + (g * d.n_in + j) * 32;
+        const uint32_t *tb = d.tbl + (g * d.n_in + j) * kTableWords;
         acc ^= __ldg(tb + (x & 15)) ^ __ldg(tb + 16 + (x >> 4));
       }
       for (uint32_t r = 0; r < 4 && g * 4 + r < d.n_out; ++r) {
@@ -270,16 +333,22 @@ __global__ void __launch_bounds__(256) k_decode_tables(DecodeTableArgs a) {
     rows[i] = v;
   }
   __syncthreads();
-  // Pack nibble tables (layout of common.hpp).
+  // Pack the lookup tables (layout of common.hpp).
   uint32_t *out = task.tbl_out;
   const int groups = (n_out + 3) / 4;
-  for (int i = threadIdx.x; i < groups * k * 32; i += blockDim.x) {
-    const int e = i & 31, j = (i >> 5) % k, g = (i >> 5) / k;
-    const uint8_t x = (e < 16) ? uint8_t(e) : uint8_t((e - 16) << 4);
+  for (int i = threadIdx.x; i < groups * k * kTableWords; i += blockDim.x) {
+    const int e = i % kTableWords, j = (i / kTableWords) % k, g = (i / kTableWords) / k;
     uint32_t word = 0;
-    for (int r = 0; r < 4; ++r) {
-      const int o = g * 4 + r;
-      if (o < n_out) word |= uint32_t(gf.mul(rows[o * k + j], x)) << (8 * r);
+    if (e < 64) {
+      const uint8_t x = e < 16 ? uint8_t(e) : e < 32 ? uint8_t((e - 16) << 4) : uint8_t(e - 32);
+      for (int r = 0; r < 4; ++r) {
+        const int o = g * 4 + r;
+        if (o < n_out) word |= uint32_t(gf.mul(rows[o * k + j], x)) << (8 * r);
+      }
+    } else {
+      const int r = (e - 64) >> 1, h0 = ((e - 64) & 1) * 4, o = g * 4 + r;
+      if (o < n_out)
+        for (int h = 0; h < 4; ++h) word |= uint32_t(gf.mul(rows[o * k + j], uint8_t((h0 + h) << 5))) << (8 * h);
     }
     out[i] = word;
   }
@@ -299,33 +368,51 @@ int grid_for(const void *fn, int threads, size_t smem) {
   return sms * per_sm;
 }
 
+template <int NG, int V, int B, int MIX, bool VERIFY>
+void launch_vec(const ApplyArgs &a, cudaStream_t s) {
+  static int grid_max = 0;
+  if (!grid_max) grid_max = grid_for((const void *)k_apply_vec<NG, V, B, MIX, VERIFY>, kApplyThreads, 0);
+  const uint64_t tile = uint64_t(kApplyThreads) * kApplyVec * V;
+  const uint64_t tiles = ((a.len + tile - 1) / tile) * a.n_jobs;
+  const int grid = int(tiles < uint64_t(grid_max) ? tiles : grid_max);
+  k_apply_vec<NG, V, B, MIX, VERIFY><<<grid, kApplyThreads, 0, s>>>(a);
+}
+
+// Tile variants the autotuner chooses from: (vectors per thread, inputs in
+// flight, lookup mix).
+template <bool VERIFY>
+void launch_variant(const ApplyArgs &a, int variant, cudaStream_t s) {
+  if (a.max_out > 4) {
+    launch_vec<2, 1, 4, 1, VERIFY>(a, s);
+    return;
+  }
+  switch (variant) {
+    case 0: launch_vec<1, 2, 4, 0, VERIFY>(a, s); break;
+    case 2: launch_vec<1, 2, 4, 2, VERIFY>(a, s); break;
+    case 3: launch_vec<1, 1, 8, 1, VERIFY>(a, s); break;
+    case 4: launch_vec<1, 1, 4, 1, VERIFY>(a, s); break;
+    default: launch_vec<1, 2, 4, 1, VERIFY>(a, s); break;
+  }
+}
+
 }  // namespace
+
+int &apply_variant() {
+  static int v = [] {
+    const char *e = getenv("RSGPU_APPLY_VARIANT");
+    return e ? atoi(e) : 1;
+  }();
+  return v;
+}
 
 cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cudaStream_t s) {
   if (a.n_jobs == 0) return cudaSuccess;
-  const uint64_t tiles = ((a.len + kApplyTile - 1) / kApplyTile) * a.n_jobs;
   uint64_t launches = 0;
-  if (tiles && a.any_vec) {
-    const void *fn;
-    if (a.max_out > 4)
-      fn = verify ? (const void *)k_apply_vec<2, true> : (const void *)k_apply_vec<2, false>;
+  if (a.any_vec && a.len >= 16) {
+    if (verify)
+      launch_variant<true>(a, apply_variant(), s);
     else
-      fn = verify ? (const void *)k_apply_vec<1, true> : (const void *)k_apply_vec<1, false>;
-    static int grid_cache[4] = {0, 0, 0, 0};
-    const int slot = (a.max_out > 4 ? 2 : 0) + (verify ? 1 : 0);
-    if (!grid_cache[slot]) grid_cache[slot] = grid_for(fn, kApplyThreads, 0);
-    const int grid = int(tiles < uint64_t(grid_cache[slot]) ? tiles : grid_cache[slot]);
-    if (a.max_out > 4) {
-      if (verify)
-        k_apply_vec<2, true><<<grid, kApplyThreads, 0, s>>>(a);
-      else
-        k_apply_vec<2, false><<<grid, kApplyThreads, 0, s>>>(a);
-    } else {
-      if (verify)
-        k_apply_vec<1, true><<<grid, kApplyThreads, 0, s>>>(a);
-      else
-        k_apply_vec<1, false><<<grid, kApplyThreads, 0, s>>>(a);
-    }
+      launch_variant<false>(a, apply_variant(), s);
     ++launches;
   }
   if (max_tail) {

@@ -18,6 +18,9 @@ struct ApplyArgs {
   int any_vec;                  // some job has vec_len > 0
 };
 cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cudaStream_t s);
+// K1 tile variant (threads x vectors-per-thread x inputs-in-flight); the
+// autotuner sets it, RSGPU_APPLY_VARIANT overrides the default.
+int &apply_variant();
 
 // K3: one erasure pattern.  Indices fit a byte because classic codecs have at
 // most 256 shards.

@@ -6,10 +6,19 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 
 namespace rsgpu {
 
 class Codec;
+
+// A prepared Leopard (or tower-field) batch: device-resident job tables whose
+// launch allocates and synchronizes nothing.
+struct LeoLaunch;
+int prepare_other(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
+                  int goal, uint32_t *flags, std::shared_ptr<LeoLaunch> &out);
+int leo_launch(const LeoLaunch &l, cudaStream_t s);
+uint32_t leo_kernel_count(const LeoLaunch &l);
 
 // src/core/leopard.rs:191-223 (resolve_codec_family) for the byte field.
 int resolve_family(int requested, int mode, size_t total, size_t parity);

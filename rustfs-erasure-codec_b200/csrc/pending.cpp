@@ -5,6 +5,10 @@
 
 namespace rsgpu {
 struct LeopardState {};
+struct LeoLaunch {};
+int prepare_other(Codec &, int, size_t, uint8_t *const *, const uint8_t *, size_t, int, uint32_t *, std::shared_ptr<LeoLaunch> &) { return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY; }
+int leo_launch(const LeoLaunch &, cudaStream_t) { return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY; }
+uint32_t leo_kernel_count(const LeoLaunch &) { return 0; }
 int Codec::init_tower() { return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY; }
 int Codec::init_leopard() { return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY; }
 int leopard_encode(Codec &, size_t, uint8_t *const *, size_t, cudaStream_t) { return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY; }

@@ -109,6 +109,11 @@ def _lib():
             "rsgpu_reconstruct_batch": (I32, [P, SZ, PP, U8P, SZ, I32, I32, P]),
             "rsgpu_verify_batch": (I32, [P, SZ, PP, SZ, U8P, I32, P]),
             "rsgpu_get_cache_stats": (I32, [P, ctypes.POINTER(CacheStats)]),
+            "rsgpu_batch_prepare": (I32, [P, I32, SZ, P, P, SZ, I32, PP]),
+            "rsgpu_batch_launch": (I32, [P, P]),
+            "rsgpu_batch_verify_result": (I32, [P, U8P, P]),
+            "rsgpu_batch_kernel_count": (ctypes.c_uint32, [P]),
+            "rsgpu_batch_free": (None, [P]),
             "rsgpu_kernel_launch_count": (ctypes.c_uint64, []),
             "rsgpu_error_string": (ctypes.c_char_p, [I32]),
             "rsgpu_version": (ctypes.c_char_p, []),
@@ -236,6 +241,55 @@ class ReconstructWorkspace:
     def __del__(self):
         if getattr(self, "_h", None):
             _lib().rsgpu_reconstruct_ws_free(self._h)
+            self._h = None
+
+
+OP = {"encode": 0, "reconstruct": 1, "verify": 2}
+
+
+def device_pointer_table(base_ptr: int, offsets) -> np.ndarray:
+    """uint64 array of base_ptr + offsets (stripe-major shard pointers)."""
+    return (np.uint64(base_ptr) + np.asarray(offsets, dtype=np.uint64)).astype(np.uint64)
+
+
+class PreparedBatch:
+    """Device-resident batch (see rsgpu_batch_prepare in include/rsgpu.h):
+    launch() is a bare kernel launch on the current torch stream."""
+
+    def __init__(self, codec: "ReedSolomon", op: str, ptr_table: np.ndarray, shard_len: int,
+                 present: Optional[np.ndarray] = None, goal: str = "all"):
+        self._codec = codec  # keep the codec alive
+        self.op = op
+        n = ptr_table.size // codec.total_shard_count()
+        self.n_stripes = n
+        self._ptrs = np.ascontiguousarray(ptr_table, np.uint64)
+        self._present = None if present is None else np.ascontiguousarray(present, np.uint8)
+        h = ctypes.c_void_p()
+        _check(_lib().rsgpu_batch_prepare(
+            codec._h, OP[op], n, self._ptrs.ctypes.data,
+            None if self._present is None else self._present.ctypes.data, shard_len, GOAL[goal],
+            ctypes.byref(h)))
+        self._h = h
+
+    def _stream(self):
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+
+    def launch(self, stream=None) -> None:
+        _check(_lib().rsgpu_batch_launch(self._h, self._stream() if stream is None else stream))
+
+    def verify_result(self) -> np.ndarray:
+        ok = np.zeros(max(1, self.n_stripes), np.uint8)
+        _check(_lib().rsgpu_batch_verify_result(self._h, ok.ctypes.data_as(U8P), self._stream()))
+        return ok[: self.n_stripes].astype(bool)
+
+    def kernel_count(self) -> int:
+        return int(_lib().rsgpu_batch_kernel_count(self._h))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib().rsgpu_batch_free(self._h)
             self._h = None
 
 
@@ -403,6 +457,10 @@ class ReedSolomon:
         pres = _flags([p for row in present for p in row], len(flat))
         _check(_lib().rsgpu_reconstruct_batch(self._h, len(stripes), ptrs, pres, lens[0] if flat else 0,
                                               GOAL[goal], mem, stream))
+
+    def prepare_batch(self, op: str, ptr_table: np.ndarray, shard_len: int, present=None,
+                      goal: str = "all") -> PreparedBatch:
+        return PreparedBatch(self, op, ptr_table, shard_len, present, goal)
 
     def verify_batch(self, stripes: Sequence[Sequence]) -> List[bool]:
         flat = [s for st in stripes for s in st]
