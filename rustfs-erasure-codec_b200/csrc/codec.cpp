@@ -136,7 +136,7 @@ int Codec::plan_classic(const uint8_t *present, int goal, const uint8_t *require
   for (size_t i = 0; i < total; ++i) {
     if (present[i]) {
       ++n_present;
-      if (p.survivors.size() < k) p.survivors.push_back(uint8_t(i));
+      if (p.survivors.size() < k) p.survivors.push_back(uint16_t(i));
     } else if (i < k) {
       ++missing_data;
     }
@@ -151,7 +151,7 @@ int Codec::plan_classic(const uint8_t *present, int goal, const uint8_t *require
     bool want = goal == RSGPU_GOAL_ALL || (goal == RSGPU_GOAL_DATA && i < k) ||
                 (goal == RSGPU_GOAL_REQUIRED && i < n_required && required[i]);
     if (!want) continue;
-    p.targets.push_back(uint8_t(i));
+    p.targets.push_back(uint16_t(i));
     if (i < k) ++p.n_data_targets;
   }
   p.needs_inverse = missing_data > 0 && !p.targets.empty();
@@ -162,8 +162,8 @@ int Codec::plan_classic(const uint8_t *present, int goal, const uint8_t *require
 static PatternKey key_of(const ClassicPlan &p, size_t k) {
   PatternKey key;
   // Survivors determine the inverse; targets determine the composed rows.
-  for (uint8_t s : p.survivors) key.present[s >> 6] |= 1ull << (s & 63);
-  for (uint8_t t : p.targets) key.targets[t >> 6] |= 1ull << (t & 63);
+  for (uint16_t s : p.survivors) key.present[s >> 6] |= 1ull << (s & 63);
+  for (uint16_t t : p.targets) key.targets[t >> 6] |= 1ull << (t & 63);
   (void)k;
   return key;
 }
@@ -198,8 +198,8 @@ int Codec::decode_tables(const std::vector<const ClassicPlan *> &plans, std::vec
     ++stats_.misses;
     DecodeTask t;
     std::memset(&t, 0, sizeof(t));
-    std::copy(p.survivors.begin(), p.survivors.end(), t.survivors);
-    std::copy(p.targets.begin(), p.targets.end(), t.targets);
+    for (size_t x = 0; x < p.survivors.size(); ++x) t.survivors[x] = uint8_t(p.survivors[x]);
+    for (size_t x = 0; x < p.targets.size(); ++x) t.targets[x] = uint8_t(p.targets[x]);
     t.n_out = uint32_t(p.targets.size());
     t.needs_inverse = p.needs_inverse;
     uint32_t *blk = pool_->get();
@@ -424,8 +424,8 @@ int Codec::reconstruct_jobs(size_t n_stripes, uint8_t *const *shards, const uint
     j.n_in = uint16_t(k);
     j.n_out = uint16_t(p.targets.size());
     j.tbl = tbls[i];
-    for (uint8_t sv : p.survivors) ptrs.push_back(shards[i * total + sv]);
-    for (uint8_t t : p.targets) ptrs.push_back(shards[i * total + t]);
+    for (uint16_t sv : p.survivors) ptrs.push_back(shards[i * total + sv]);
+    for (uint16_t t : p.targets) ptrs.push_back(shards[i * total + t]);
     jobs.push_back(j);
   }
   return RSGPU_OK;

@@ -29,8 +29,8 @@ struct ClassicPlan {
   int status = RSGPU_OK;
   bool all_present = false;
   bool needs_inverse = false;
-  std::vector<uint8_t> survivors;  // first k present indices
-  std::vector<uint8_t> targets;    // requested missing indices, ascending
+  std::vector<uint16_t> survivors;  // first k present indices
+  std::vector<uint16_t> targets;    // requested missing indices, ascending
   size_t n_data_targets = 0;
 };
 
@@ -53,8 +53,8 @@ struct PatternKeyHash {
 
 struct DecodeEntry {
   uint32_t *tbl = nullptr;  // device, packed tables (block of the table pool)
-  std::vector<uint8_t> survivors;
-  std::vector<uint8_t> targets;
+  std::vector<uint16_t> survivors;
+  std::vector<uint16_t> targets;
   std::list<PatternKey>::iterator lru;
 };
 
@@ -77,6 +77,7 @@ class TablePool {
 };
 
 struct LeopardState;  // leopard.cu
+struct TowerState;    // tower.cu
 
 // A K1 launch whose job and pointer tables live in device memory.  Built once
 // and launched any number of times (launch() allocates and synchronizes
@@ -107,6 +108,7 @@ class Codec {
   uint8_t *d_log = nullptr, *d_exp = nullptr;
   uint32_t *d_enc_tbl = nullptr;  // parity rows packed for K1
   std::shared_ptr<LeopardState> leo;  // created where the type is complete
+  std::shared_ptr<TowerState> tower;
 
   ~Codec();
   int init_classic(const uint8_t *custom_rows);

@@ -1,0 +1,972 @@
+// leopard.cu -- Leopard FFT codecs over GF(2^8) and GF(2^16) on sm_100a.
+//
+// Every column of a shard is independent, so a CTA owns a tile of columns of
+// one stripe and holds *all* transform lanes of that tile in shared memory:
+// shards cross HBM exactly once (data in, parity or recovered shards out) and
+// every IFFT / formal-derivative / FFT layer runs on chip.  A lane row is one
+// 64-byte block (64 GF(2^8) columns, or 32 GF(2^16) columns in the
+// reference's split byte layout, src/core/leopard_gf16/ops.rs:513-807) and is
+// owned by one half-warp: 16 lanes x one 32-bit word.  Multiplication by a
+// butterfly constant g^log_m uses nibble tables held one entry per lane and
+// read with width-16 warp shuffles, so the two halves of a warp can work on
+// different butterflies with different constants.
+//
+// Kernels:
+//  K4/K6 k_leo_encode  grouped IFFT -> XOR-accumulate -> FFT
+//                      (src/core/leopard_gf8/encode.rs:194-372,
+//                       src/core/leopard_gf16/encode.rs:109-252)
+//  K5/K7 k_leo_decode  err-locator scaling -> IFFT -> formal derivative ->
+//                      FFT -> inverse scaling
+//                      (src/core/leopard_gf8/decode.rs:291-420,
+//                       src/core/leopard_gf16/decode.rs:704-910)
+//  K7a   k_leo_locator FWHT error locator, one CTA per erasure pattern
+//                      (src/core/leopard_gf16/decode.rs:177-216,
+//                       src/core/leopard_gf8/decode.rs:58-113)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "codec.hpp"
+#include "leopard.hpp"
+
+namespace rsgpu {
+
+#define RS_CUDA(expr)                              \
+  do {                                             \
+    cudaError_t e_ = (expr);                       \
+    if (e_ != cudaSuccess) return cuda_status(e_); \
+  } while (0)
+
+// ====================================================================== tables
+namespace {
+
+size_t pow2_at_least(size_t n) {
+  size_t p = 1;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+// Leopard field tables (src/core/leopard_gf8/tables.rs:8-145,
+// src/core/leopard_gf16/tables.rs:8-116): exp by LFSR over the field
+// polynomial, log through the Cantor basis, the FFT skew factors and the
+// Walsh transform of the log table.
+struct LeoTables {
+  int bits = 0;
+  uint32_t order = 0, mod = 0;
+  std::vector<uint16_t> log, exp, skew, walsh;
+
+  uint16_t add_mod(uint32_t a, uint32_t b) const {
+    const uint32_t s = a + b;
+    return uint16_t((s + (s >> bits)) & (order - 1));
+  }
+  uint16_t sub_mod(uint32_t a, uint32_t b) const {
+    const uint64_t d = uint64_t(a) - uint64_t(b);
+    return uint16_t((d + (d >> bits)) & (order - 1));
+  }
+  uint16_t mul_log(uint16_t a, uint16_t log_b) const {
+    return a == 0 ? 0 : exp[add_mod(log[a], log_b)];
+  }
+
+  void fwht(std::vector<uint16_t> &d, size_t mtrunc) const {
+    for (size_t dist = 1, dist4 = 4; dist4 <= order; dist = dist4, dist4 <<= 2)
+      for (size_t r = 0; r < mtrunc; r += dist4)
+        for (size_t off = r; off < r + dist; ++off) {
+          uint16_t *p = d.data();
+          uint16_t t0 = add_mod(p[off], p[off + dist]), t1 = sub_mod(p[off], p[off + dist]);
+          uint16_t t2 = add_mod(p[off + 2 * dist], p[off + 3 * dist]);
+          uint16_t t3 = sub_mod(p[off + 2 * dist], p[off + 3 * dist]);
+          p[off] = add_mod(t0, t2);
+          p[off + 2 * dist] = sub_mod(t0, t2);
+          p[off + dist] = add_mod(t1, t3);
+          p[off + 3 * dist] = sub_mod(t1, t3);
+        }
+  }
+
+  explicit LeoTables(int b) : bits(b), order(1u << b), mod((1u << b) - 1) {
+    static const uint16_t cantor8[8] = {1, 214, 152, 146, 86, 200, 88, 230};
+    static const uint16_t cantor16[16] = {0x0001, 0xACCA, 0x3C0E, 0x163E, 0xC582, 0xED2E, 0x914C, 0x4012,
+                                          0x6C98, 0x10D8, 0x6A72, 0xB900, 0xFDB8, 0xFB34, 0xFF38, 0x991E};
+    const uint16_t *cantor = b == 8 ? cantor8 : cantor16;
+    const uint32_t poly = b == 8 ? 0x11D : 0x1002D;
+    log.assign(order, 0);
+    exp.assign(b == 8 ? order : 2 * order, 0);
+    uint32_t state = 1;
+    for (uint32_t i = 0; i < mod; ++i) {
+      exp[state] = uint16_t(i);
+      state <<= 1;
+      if (state >= order) state ^= poly;
+    }
+    exp[0] = uint16_t(mod);
+    log[0] = 0;
+    for (int i = 0; i < b; ++i) {
+      const uint32_t width = 1u << i;
+      for (uint32_t j = 0; j < width; ++j) log[j + width] = log[j] ^ cantor[i];
+    }
+    for (uint32_t i = 0; i < order; ++i) log[i] = exp[log[i]];
+    for (uint32_t i = 0; i < order; ++i) exp[log[i]] = uint16_t(i);
+    exp[mod] = exp[0];
+
+    skew.assign(mod, 0);
+    std::vector<uint16_t> temp(b - 1);
+    for (int i = 1; i < b; ++i) temp[i - 1] = uint16_t(1u << i);
+    for (int mm = 0; mm < b - 1; ++mm) {
+      const size_t step = size_t(1) << (mm + 1);
+      skew[(size_t(1) << mm) - 1] = 0;
+      for (int i = mm; i < b - 1; ++i) {
+        const size_t s = size_t(1) << (i + 1);
+        for (size_t j = (size_t(1) << mm) - 1; j < s; j += step) skew[j + s] = skew[j] ^ temp[i];
+      }
+      const uint16_t prod = mul_log(temp[mm], log[temp[mm] ^ 1]);
+      temp[mm] = uint16_t(mod - log[prod]);
+      for (int i = mm + 1; i < b - 1; ++i) temp[i] = mul_log(temp[i], add_mod(log[temp[i] ^ 1], temp[mm]));
+    }
+    for (uint32_t i = 0; i < mod; ++i) skew[i] = log[skew[i]];
+    walsh.assign(order, 0);
+    for (uint32_t i = 0; i < order; ++i) walsh[i] = log[i];
+    walsh[0] = 0;
+    fwht(walsh, order);
+  }
+};
+
+}  // namespace
+
+// Device-resident constants of one Leopard field, shared by every codec.
+struct LeoField {
+  int bits;
+  LeoTables host;
+  uint16_t *d_skew = nullptr;
+  uint16_t *d_walsh = nullptr;
+  uint32_t *d_bank = nullptr;  // multiplier tables indexed by log value
+  explicit LeoField(int b) : bits(b), host(b) {}
+};
+
+static int leo_field(int bits, LeoField **out) {
+  static std::mutex mu;
+  static LeoField *fields[2] = {nullptr, nullptr};
+  std::lock_guard<std::mutex> g(mu);
+  const int slot = bits == 8 ? 0 : 1;
+  if (!fields[slot]) {
+    LeoField *f = new LeoField(bits);
+    const LeoTables &t = f->host;
+    RS_CUDA(cudaMalloc(&f->d_skew, t.skew.size() * 2));
+    RS_CUDA(cudaMemcpy(f->d_skew, t.skew.data(), t.skew.size() * 2, cudaMemcpyHostToDevice));
+    RS_CUDA(cudaMalloc(&f->d_walsh, t.walsh.size() * 2));
+    RS_CUDA(cudaMemcpy(f->d_walsh, t.walsh.data(), t.walsh.size() * 2, cudaMemcpyHostToDevice));
+    // Bank: for each log value, 16 lanes x (GF8: 2 words, GF16: 4 words).
+    // GF8 word pair: c*n and c*(n<<4) replicated into all four bytes.
+    // GF16 words k=0..3: c*(n << 4k) replicated into both 16-bit halves.
+    const uint32_t words = bits == 8 ? 2 : 4;
+    std::vector<uint32_t> bank(size_t(t.order) * 16 * words);
+    for (uint32_t lm = 0; lm < t.order; ++lm)
+      for (uint32_t n = 0; n < 16; ++n) {
+        uint32_t *e = &bank[(size_t(lm) * 16 + n) * words];
+        if (bits == 8) {
+          e[0] = uint32_t(t.mul_log(uint16_t(n), uint16_t(lm))) * 0x01010101u;
+          e[1] = uint32_t(t.mul_log(uint16_t(n << 4), uint16_t(lm))) * 0x01010101u;
+        } else {
+          for (uint32_t k = 0; k < 4; ++k) e[k] = uint32_t(t.mul_log(uint16_t(n << (4 * k)), uint16_t(lm))) * 0x10001u;
+        }
+      }
+    RS_CUDA(cudaMalloc(&f->d_bank, bank.size() * 4));
+    RS_CUDA(cudaMemcpy(f->d_bank, bank.data(), bank.size() * 4, cudaMemcpyHostToDevice));
+    fields[slot] = f;
+  }
+  *out = fields[slot];
+  return RSGPU_OK;
+}
+
+// ====================================================================== device
+namespace {
+
+constexpr int kLeoThreads = 512;
+constexpr int kHalfWarps = kLeoThreads / 16;
+constexpr int kRowWords = 16;  // one 64-byte block per lane row
+
+struct LeoJob {
+  uint32_t ptr_off;    // into the pointer table: k + p shard pointers
+  uint32_t flag_idx;   // verify flag
+  const uint16_t *err; // decode: error locators (n entries)
+  const uint8_t *role; // decode: per shard 0 absent, 1 present (input), 2 target (output)
+  uint32_t input_count;
+  uint32_t pad;
+};
+
+struct LeoArgs {
+  const LeoJob *jobs;
+  const uint8_t *const *ptrs;
+  const uint16_t *skew;
+  const uint32_t *bank;
+  uint32_t *flags;
+  uint32_t *scratch;  // global work rows when the lanes do not fit on chip
+  uint64_t len;       // bytes per shard (multiple of 64)
+  uint32_t n_jobs;
+  uint32_t k, p, m, n;  // n: decode lanes (pow2 >= m + k)
+  uint32_t mtrunc, last;
+  uint32_t nb;        // 64-byte column blocks per tile
+  uint32_t lanes;     // rows per tile (encode 2m, decode n)
+  uint32_t mod;
+};
+
+template <int BITS>
+struct Tab;
+template <>
+struct Tab<8> {
+  uint32_t lo, hi;
+};
+template <>
+struct Tab<16> {
+  uint32_t t0, t1, t2, t3;
+};
+
+__device__ __forceinline__ uint32_t shfl16(uint32_t v, uint32_t idx) {
+  uint32_t r;
+  asm("shfl.sync.idx.b32 %0, %1, %2, 0x101f, -1;" : "=r"(r) : "r"(v), "r"(idx));
+  return r;
+}
+
+template <int BITS>
+__device__ __forceinline__ Tab<BITS> load_tab(const uint32_t *bank, uint32_t lm, uint32_t hl);
+template <>
+__device__ __forceinline__ Tab<8> load_tab<8>(const uint32_t *bank, uint32_t lm, uint32_t hl) {
+  const uint2 v = __ldg(reinterpret_cast<const uint2 *>(bank) + lm * 16 + hl);
+  return Tab<8>{v.x, v.y};
+}
+template <>
+__device__ __forceinline__ Tab<16> load_tab<16>(const uint32_t *bank, uint32_t lm, uint32_t hl) {
+  const uint4 v = __ldg(reinterpret_cast<const uint4 *>(bank) + lm * 16 + hl);
+  return Tab<16>{v.x, v.y, v.z, v.w};
+}
+
+// Products of the elements of word w with the half-warp's constant.
+__device__ __forceinline__ uint32_t mulw(uint32_t w, const Tab<8> &t) {
+  const uint32_t s0 = shfl16(t.lo, w) ^ shfl16(t.hi, w >> 4);
+  const uint32_t s1 = shfl16(t.lo, w >> 8) ^ shfl16(t.hi, w >> 12);
+  const uint32_t s2 = shfl16(t.lo, w >> 16) ^ shfl16(t.hi, w >> 20);
+  const uint32_t s3 = shfl16(t.lo, w >> 24) ^ shfl16(t.hi, w >> 28);
+  return __byte_perm(__byte_perm(s0, s1, 0x0040), __byte_perm(s2, s3, 0x4000), 0x7610);
+}
+__device__ __forceinline__ uint32_t mulw(uint32_t w, const Tab<16> &t) {
+  const uint32_t a = shfl16(t.t0, w) ^ shfl16(t.t1, w >> 4) ^ shfl16(t.t2, w >> 8) ^ shfl16(t.t3, w >> 12);
+  const uint32_t b = shfl16(t.t0, w >> 16) ^ shfl16(t.t1, w >> 20) ^ shfl16(t.t2, w >> 24) ^ shfl16(t.t3, w >> 28);
+  return __byte_perm(a, b, 0x7610);
+}
+
+// Split-layout conversion of a 64-byte GF(2^16) block held as 16 words by a
+// half-warp (word t = bytes 4t..4t+3 of the block).
+__device__ __forceinline__ uint32_t user_to_work16(uint32_t w, uint32_t hl) {
+  const uint32_t other = __shfl_xor_sync(0xffffffffu, w, 8, 16);
+  return hl < 8 ? __byte_perm(w, other, 0x5140) : __byte_perm(other, w, 0x7362);
+}
+__device__ __forceinline__ uint32_t work_to_user16(uint32_t w, uint32_t hl) {
+  const uint32_t other = __shfl_xor_sync(0xffffffffu, w, 8, 16);
+  return hl < 8 ? __byte_perm(w, other, 0x6420) : __byte_perm(other, w, 0x7531);
+}
+
+template <int BITS>
+__device__ __forceinline__ uint32_t from_user(uint32_t w, uint32_t hl) {
+  return BITS == 16 ? user_to_work16(w, hl) : w;
+}
+template <int BITS>
+__device__ __forceinline__ uint32_t to_user(uint32_t w, uint32_t hl) {
+  return BITS == 16 ? work_to_user16(w, hl) : w;
+}
+
+// Row r, column block cb: 16 words.
+__device__ __forceinline__ uint32_t *row_ptr(uint32_t *W, uint32_t nb, uint32_t r, uint32_t cb) {
+  return W + (size_t(r) * nb + cb) * kRowWords;
+}
+
+// dit2 on rows x, y of column block cb (forward: x ^= y*c, y ^= x;
+// inverse: y ^= x, x ^= y*c; log_m == mod means only y ^= x).  Both
+// half-warps always execute the shuffles; `valid` gates the stores.
+template <int BITS, bool FWD>
+__device__ __forceinline__ void dit2(uint32_t *W, uint32_t nb, uint32_t cb, uint32_t x, uint32_t y, uint32_t lm,
+                                     const Tab<BITS> &t, uint32_t mod, bool valid, uint32_t hl) {
+  uint32_t *px = row_ptr(W, nb, valid ? x : 0, cb) + hl;
+  uint32_t *py = row_ptr(W, nb, valid ? y : 0, cb) + hl;
+  uint32_t xv = *px, yv = *py;
+  const bool skip = lm == mod;
+  if (FWD) {
+    const uint32_t prod = mulw(yv, t);
+    if (!skip) xv ^= prod;
+    yv ^= xv;
+  } else {
+    yv ^= xv;
+    const uint32_t prod = mulw(yv, t);
+    if (!skip) xv ^= prod;
+  }
+  if (valid) {
+    *px = xv;
+    *py = yv;
+  }
+}
+
+// One radix-4 layer over lanes [0, nl): blocks r < mtrunc step 4*dist, each
+// spanning lanes i, i+dist, i+2dist, i+3dist for i in [r, r+dist).
+// Skew factors: sk[iend + adj], sk[iend + dist + adj], sk[iend + 2dist + adj].
+template <int BITS, bool FWD>
+__device__ void layer4(uint32_t *W, const LeoArgs &a, const uint16_t *sk, int adj, uint32_t nl, uint32_t mtrunc,
+                       uint32_t dist) {
+  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const uint32_t dist4 = dist * 4;
+  const uint32_t nblk = (mtrunc + dist4 - 1) / dist4;
+  const uint32_t items = nblk * dist * a.nb;
+  const uint32_t rounds = (items + kHalfWarps - 1) / kHalfWarps;
+  for (uint32_t rd = 0; rd < rounds; ++rd) {
+    const uint32_t q = rd * kHalfWarps + hw;
+    const bool valid = q < items;
+    const uint32_t qq = valid ? q : 0;
+    const uint32_t cb = qq % a.nb, bq = qq / a.nb;
+    const uint32_t r = (bq / dist) * dist4, i = r + bq % dist;
+    const uint32_t iend = r + dist;
+    const uint32_t m01 = sk[int(iend) + adj], m02 = sk[int(iend + dist) + adj], m23 = sk[int(iend + 2 * dist) + adj];
+    const Tab<BITS> t01 = load_tab<BITS>(a.bank, m01, hl);
+    const Tab<BITS> t23 = load_tab<BITS>(a.bank, m23, hl);
+    const Tab<BITS> t02 = load_tab<BITS>(a.bank, m02, hl);
+    const uint32_t ia = i, ib = i + dist, ic = i + 2 * dist, id = i + 3 * dist;
+    const bool ha = ia < nl, hb = ib < nl, hc = ic < nl, hd = id < nl;
+    if (FWD) {
+      dit2<BITS, true>(W, a.nb, cb, ia, ic, m02, t02, a.mod, valid && ha && hc, hl);
+      dit2<BITS, true>(W, a.nb, cb, ib, id, m02, t02, a.mod, valid && hb && hd, hl);
+      dit2<BITS, true>(W, a.nb, cb, ia, ib, m01, t01, a.mod, valid && ha && hb, hl);
+      dit2<BITS, true>(W, a.nb, cb, ic, id, m23, t23, a.mod, valid && hc && hd, hl);
+    } else {
+      dit2<BITS, false>(W, a.nb, cb, ia, ib, m01, t01, a.mod, valid && ha && hb, hl);
+      dit2<BITS, false>(W, a.nb, cb, ic, id, m23, t23, a.mod, valid && hc && hd, hl);
+      dit2<BITS, false>(W, a.nb, cb, ia, ic, m02, t02, a.mod, valid && ha && hc, hl);
+      dit2<BITS, false>(W, a.nb, cb, ib, id, m02, t02, a.mod, valid && hb && hd, hl);
+    }
+  }
+}
+
+// Final radix-2 layer: pairs (i, i + dist) for i in [0, count), constant per pair.
+template <int BITS, bool FWD>
+__device__ void layer2(uint32_t *W, const LeoArgs &a, uint32_t nl, uint32_t count, uint32_t dist, uint32_t stride,
+                       const uint16_t *lm_of, int lm_fixed) {
+  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const uint32_t items = count * a.nb;
+  const uint32_t rounds = (items + kHalfWarps - 1) / kHalfWarps;
+  for (uint32_t rd = 0; rd < rounds; ++rd) {
+    const uint32_t q = rd * kHalfWarps + hw;
+    const bool valid = q < items;
+    const uint32_t qq = valid ? q : 0;
+    const uint32_t cb = qq % a.nb, i = (qq / a.nb) * stride;
+    const uint32_t lm = lm_fixed >= 0 ? uint32_t(lm_fixed) : lm_of[i];
+    const Tab<BITS> t = load_tab<BITS>(a.bank, lm, hl);
+    dit2<BITS, FWD>(W, a.nb, cb, i, i + dist, lm, t, a.mod, valid && i + dist < nl, hl);
+  }
+}
+
+// Encoder IFFT (src/core/leopard_gf16/mod.rs build_ifft_dit16_plan): lanes >=
+// mtrunc hold zeros, skew base = fft_skew + (m - 1) + group offset.
+template <int BITS>
+__device__ void ifft_encoder(uint32_t *W, const LeoArgs &a, const uint16_t *sk, uint32_t mtrunc) {
+  const uint32_t m = a.m;
+  uint32_t dist = 1, dist4 = 4;
+  while (dist4 <= m) {
+    layer4<BITS, false>(W, a, sk, 0, m, mtrunc, dist);
+    __syncthreads();
+    dist = dist4;
+    dist4 <<= 2;
+  }
+  if (dist < m) {
+    layer2<BITS, false>(W, a, m, dist, dist, 1, nullptr, sk[dist]);
+    __syncthreads();
+  }
+}
+
+// FFT (build_fft_dit16_plan): skew = fft_skew, i_end - 1 indexing.
+template <int BITS>
+__device__ void fft(uint32_t *W, const LeoArgs &a, uint32_t nl, uint32_t mtrunc, uint32_t msize) {
+  uint32_t dist4 = msize, dist = msize >> 2;
+  while (dist != 0) {
+    layer4<BITS, true>(W, a, a.skew, -1, nl, mtrunc, dist);
+    __syncthreads();
+    dist4 = dist;
+    dist >>= 2;
+  }
+  if (dist4 == 2) {
+    layer2<BITS, true>(W, a, nl, (mtrunc + 1) / 2, 1, 2, a.skew, -1);
+    __syncthreads();
+  }
+}
+
+// Decoder IFFT (build_ifft_decode_dit16_plan): blocks r < input_count.
+template <int BITS>
+__device__ void ifft_decoder(uint32_t *W, const LeoArgs &a, uint32_t mtrunc) {
+  const uint32_t n = a.n;
+  uint32_t dist = 1, dist4 = 4;
+  while (dist4 <= n) {
+    layer4<BITS, false>(W, a, a.skew, -1, n, mtrunc, dist);
+    __syncthreads();
+    dist = dist4;
+    dist4 <<= 2;
+  }
+  if (dist < n) {
+    layer2<BITS, false>(W, a, n, dist, dist, 1, nullptr, a.skew[dist - 1]);
+    __syncthreads();
+  }
+}
+
+// Formal derivative (decode.rs compute_formal_derivative16): lane l gains the
+// XOR of lanes l + 2^t for every zero bit t of l with l + 2^t < n.  Lanes
+// are rewritten in increasing order in rounds, so every read sees the value
+// from before the pass.
+__device__ void derivative(uint32_t *W, const LeoArgs &a) {
+  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const uint32_t items = a.n * a.nb;
+  for (uint32_t base = 0; base < items; base += kHalfWarps) {
+    const uint32_t q = base + hw;
+    uint32_t v = 0;
+    const bool valid = q < items;
+    uint32_t l = 0, cb = 0;
+    if (valid) {
+      l = q / a.nb;
+      cb = q % a.nb;
+      v = row_ptr(W, a.nb, l, cb)[hl];
+      for (uint32_t w = 1; l + w < a.n; w <<= 1)
+        if (!(l & w)) v ^= row_ptr(W, a.nb, l + w, cb)[hl];
+    }
+    __syncthreads();
+    if (valid) row_ptr(W, a.nb, l, cb)[hl] = v;
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ uint32_t ld_u32(const uint8_t *p) {
+  return __ldg(reinterpret_cast<const uint32_t *>(p));
+}
+
+template <int BITS, bool VERIFY, bool GLOBAL_WORK>
+__global__ void __launch_bounds__(kLeoThreads) k_leo_encode(LeoArgs a) {
+  extern __shared__ uint32_t smem[];
+  uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
+  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const uint32_t m = a.m;
+  uint32_t *acc = W, *tmp = W + size_t(m) * a.nb * kRowWords;
+  const uint64_t tile_bytes = uint64_t(a.nb) * 64;
+  const uint32_t tiles_per_job = uint32_t((a.len + tile_bytes - 1) / tile_bytes);
+  const uint32_t total = tiles_per_job * a.n_jobs;
+  __shared__ uint32_t bad;
+  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+    const uint32_t job = t / tiles_per_job;
+    const uint64_t col0 = uint64_t(t - job * tiles_per_job) * tile_bytes;
+    const LeoJob jd = a.jobs[job];
+    const uint8_t *const *ptr = a.ptrs + jd.ptr_off;
+    if (threadIdx.x == 0) bad = 0;
+    // Each group of m data shards passes through an IFFT and is XORed into acc.
+    for (uint32_t g = 0; g * m < a.k; ++g) {
+      uint32_t *dst = g == 0 ? acc : tmp;
+      const uint32_t cnt = g == 0 ? a.mtrunc : (a.k - g * m < m ? a.k - g * m : m);
+      // Rounds keep both halves of every warp in step (the layout shuffle
+      // needs all 32 lanes).
+      for (uint32_t base = 0; base < m * a.nb; base += kHalfWarps) {
+        const uint32_t q = base + hw;
+        const bool valid = q < m * a.nb;
+        const uint32_t l = valid ? q / a.nb : 0, cb = valid ? q % a.nb : 0;
+        const uint64_t col = col0 + uint64_t(cb) * 64;
+        uint32_t v = 0;
+        if (valid && l < cnt && col < a.len) v = ld_u32(ptr[g * m + l] + col + hl * 4);
+        v = from_user<BITS>(v, hl);
+        if (valid) row_ptr(dst, a.nb, l, cb)[hl] = v;
+      }
+      __syncthreads();
+      const uint16_t *sk = a.skew + (m - 1) + g * m;
+      ifft_encoder<BITS>(dst, a, sk, cnt);
+      if (g > 0) {
+        for (uint32_t i = threadIdx.x; i < m * a.nb * kRowWords; i += kLeoThreads) acc[i] ^= tmp[i];
+        __syncthreads();
+      }
+    }
+    fft<BITS>(acc, a, m, a.p, m);
+    // Parity lanes 0..p back to user layout (or compared against the stored parity).
+    uint32_t mismatch = 0;
+    for (uint32_t base = 0; base < a.p * a.nb; base += kHalfWarps) {
+      const uint32_t q = base + hw;
+      const bool valid = q < a.p * a.nb;
+      const uint32_t l = valid ? q / a.nb : 0, cb = valid ? q % a.nb : 0;
+      const uint64_t col = col0 + uint64_t(cb) * 64;
+      const uint32_t v = to_user<BITS>(row_ptr(acc, a.nb, l, cb)[hl], hl);
+      if (valid && col < a.len) {
+        uint32_t *out = reinterpret_cast<uint32_t *>(const_cast<uint8_t *>(ptr[a.k + l]) + col) + hl;
+        if (VERIFY)
+          mismatch |= (*out != v);
+        else
+          *out = v;
+      }
+    }
+    if (VERIFY) {
+      if (mismatch) atomicOr(&bad, 1u);
+      __syncthreads();
+      if (threadIdx.x == 0 && bad) atomicOr(a.flags + jd.flag_idx, 1u);
+    }
+    __syncthreads();
+  }
+}
+
+template <int BITS, bool GLOBAL_WORK>
+__global__ void __launch_bounds__(kLeoThreads) k_leo_decode(LeoArgs a) {
+  extern __shared__ uint32_t smem[];
+  uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
+  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const uint32_t m = a.m, n = a.n, k = a.k, p = a.p;
+  const uint64_t tile_bytes = uint64_t(a.nb) * 64;
+  const uint32_t tiles_per_job = uint32_t((a.len + tile_bytes - 1) / tile_bytes);
+  const uint32_t total = tiles_per_job * a.n_jobs;
+  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+    const uint32_t job = t / tiles_per_job;
+    const uint64_t col0 = uint64_t(t - job * tiles_per_job) * tile_bytes;
+    const LeoJob jd = a.jobs[job];
+    const uint8_t *const *ptr = a.ptrs + jd.ptr_off;
+    // Step 1: lanes 0..p parity, m..m+k data; present lanes scaled by their
+    // error locator, everything else zero.
+    for (uint32_t base = 0; base < n * a.nb; base += kHalfWarps) {
+      const uint32_t q = base + hw;
+      const bool valid = q < n * a.nb;
+      const uint32_t l = valid ? q / a.nb : 0, cb = valid ? q % a.nb : 0;
+      const uint64_t col = col0 + uint64_t(cb) * 64;
+      int shard = -1;
+      if (l < p)
+        shard = int(k + l);
+      else if (l >= m && l < m + k)
+        shard = int(l - m);
+      const bool load = valid && shard >= 0 && jd.role[shard] == 1 && col < a.len;
+      uint32_t v = 0;
+      if (load) v = ld_u32(ptr[shard] + col + hl * 4);
+      // Every half-warp converts and multiplies (shuffles must stay
+      // converged); unused rows multiply zero by the identity.
+      v = from_user<BITS>(v, hl);
+      const uint32_t lm = load ? jd.err[l] : a.mod;
+      const Tab<BITS> tb = load_tab<BITS>(a.bank, lm, hl);
+      v = mulw(v, tb);
+      if (valid) row_ptr(W, a.nb, l, cb)[hl] = v;
+    }
+    __syncthreads();
+    ifft_decoder<BITS>(W, a, jd.input_count);
+    derivative(W, a);
+    fft<BITS>(W, a, n, m + k, n);
+    // Step 5: each target scaled by mod - err and written in user layout.
+    for (uint32_t base = 0; base < (k + p) * a.nb; base += kHalfWarps) {
+      const uint32_t q = base + hw;
+      const bool valid = q < (k + p) * a.nb;
+      const uint32_t i = valid ? q / a.nb : 0, cb = valid ? q % a.nb : 0;
+      const uint64_t col = col0 + uint64_t(cb) * 64;
+      const bool target = valid && jd.role[i] == 2;
+      const uint32_t lane = i >= k ? i - k : m + i;
+      const uint32_t lm = target ? (a.mod - jd.err[lane]) : a.mod;
+      const Tab<BITS> tb = load_tab<BITS>(a.bank, lm, hl);
+      const uint32_t v = to_user<BITS>(mulw(row_ptr(W, a.nb, lane, cb)[hl], tb), hl);
+      if (target && col < a.len)
+        reinterpret_cast<uint32_t *>(const_cast<uint8_t *>(ptr[i]) + col)[hl] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// K7a: one CTA per erasure pattern.  data[] = indicator of erased positions
+// (parity i at i, padding p..m, data j at m + j), FWHT limited to blocks below
+// work_size, times log_walsh mod (2^bits - 1), full FWHT; err = first n values.
+template <int BITS>
+__global__ void __launch_bounds__(1024) k_leo_locator(const uint8_t *const *presents, uint16_t *const *outs,
+                                                      const uint16_t *walsh, uint32_t k, uint32_t p, uint32_t m,
+                                                      uint32_t n) {
+  extern __shared__ uint16_t d[];
+  constexpr uint32_t order = 1u << BITS, mod = order - 1;
+  const uint8_t *present = presents[blockIdx.x];
+  for (uint32_t i = threadIdx.x; i < order; i += blockDim.x) {
+    uint16_t v = 0;
+    if (i < p)
+      v = present[k + i] ? 0 : 1;
+    else if (i < m)
+      v = 1;
+    else if (i < m + k)
+      v = present[i - m] ? 0 : 1;
+    d[i] = v;
+  }
+  __syncthreads();
+  auto add = [](uint32_t x, uint32_t y) -> uint32_t {
+    const uint32_t s = x + y;
+    return (s + (s >> BITS)) & mod;
+  };
+  auto sub = [](uint32_t x, uint32_t y) -> uint32_t {
+    const uint32_t df = x - y;
+    return (df + (df >> BITS)) & mod;
+  };
+  for (int pass = 0; pass < 2; ++pass) {
+    const uint32_t mtrunc = pass == 0 ? m + k : order;
+    for (uint32_t dist = 1, dist4 = 4; dist4 <= order; dist = dist4, dist4 <<= 2) {
+      const uint32_t nblk = (mtrunc + dist4 - 1) / dist4;
+      for (uint32_t q = threadIdx.x; q < nblk * dist; q += blockDim.x) {
+        const uint32_t off = (q / dist) * dist4 + q % dist;
+        const uint32_t a0 = d[off], a1 = d[off + dist], a2 = d[off + 2 * dist], a3 = d[off + 3 * dist];
+        const uint32_t t0 = add(a0, a1), t1 = sub(a0, a1), t2 = add(a2, a3), t3 = sub(a2, a3);
+        d[off] = uint16_t(add(t0, t2));
+        d[off + 2 * dist] = uint16_t(sub(t0, t2));
+        d[off + dist] = uint16_t(add(t1, t3));
+        d[off + 3 * dist] = uint16_t(sub(t1, t3));
+      }
+      __syncthreads();
+    }
+    if (pass == 0) {
+      for (uint32_t i = threadIdx.x; i < order; i += blockDim.x)
+        if (d[i]) d[i] = uint16_t((uint64_t(d[i]) * walsh[i]) % mod);
+      __syncthreads();
+    }
+  }
+  uint16_t *out = outs[blockIdx.x];
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = d[i];
+}
+
+}  // namespace
+
+// ====================================================================== host
+struct LeoPlan {
+  uint16_t *err = nullptr;  // device, n entries
+  uint32_t input_count = 0;
+};
+
+struct LeopardState {
+  LeoField *field = nullptr;
+  uint32_t m = 0, n = 0, mtrunc = 0, last = 0;
+  std::mutex mu;
+  std::unordered_map<std::string, LeoPlan> plans;
+  std::vector<void *> owned;
+  uint32_t *scratch = nullptr;  // global work rows for the decode of very wide codes
+  size_t scratch_bytes = 0;
+  ~LeopardState() {
+    cudaDeviceSynchronize();
+    for (auto &kv : plans) cudaFree(kv.second.err);
+    if (scratch) cudaFree(scratch);
+  }
+};
+
+struct LeoLaunch {
+  Codec *codec = nullptr;
+  bool decode = false, verify = false;
+  LeoArgs args{};
+  void *d_blob = nullptr;  // jobs | pointers | roles
+  int grid = 0;
+  size_t smem = 0;
+  bool global_work = false;
+  ~LeoLaunch() {
+    if (d_blob) cudaFree(d_blob);
+  }
+};
+
+int Codec::init_leopard() {
+  RS_CUDA(cudaGetDevice(&device));
+  auto st = std::make_shared<LeopardState>();
+  int rc = leo_field(family == RSGPU_FAMILY_LEOPARD_GF8 ? 8 : 16, &st->field);
+  if (rc) return rc;
+  st->m = uint32_t(pow2_at_least(m));
+  st->n = uint32_t(pow2_at_least(st->m + k));
+  st->mtrunc = uint32_t(std::min<size_t>(k, st->m));
+  st->last = uint32_t(k % st->m);
+  const uint32_t mod = st->field->host.mod;
+  if (st->m > mod) return RSGPU_ERR_TOO_MANY_SHARDS;
+  leo = st;
+  return RSGPU_OK;
+}
+
+namespace {
+
+constexpr size_t kSmemBudget = 200 * 1024;
+
+// Column blocks per tile: enough rows of work per CTA without exceeding the
+// shared-memory budget.
+uint32_t pick_nb(uint32_t lanes, size_t len) {
+  const size_t row = 64;
+  uint32_t nb = 1;
+  while (nb < 16 && size_t(lanes) * (nb * 2) * row <= 96 * 1024 && size_t(nb * 2) * 64 <= len) nb *= 2;
+  return nb;
+}
+
+int sm_count() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  return sms;
+}
+
+template <class K>
+int configure(const K kernel, LeoLaunch &L, uint32_t lanes, size_t len, uint64_t tiles) {
+  LeopardState &st = *L.codec->leo;
+  uint32_t nb = pick_nb(lanes, len);
+  size_t smem = size_t(lanes) * nb * 64;
+  L.global_work = smem > kSmemBudget;
+  L.args.nb = nb;
+  L.args.lanes = lanes;
+  if (!L.global_work) {
+    L.smem = smem;
+    if (smem > 48 * 1024) RS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int per_sm = 0;
+    RS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kLeoThreads, smem));
+    L.grid = int(std::min<uint64_t>(tiles, uint64_t(std::max(per_sm, 1)) * sm_count()));
+  } else {
+    // Work rows in a device slab: one region per resident CTA.
+    L.smem = 0;
+    L.grid = int(std::min<uint64_t>(tiles, uint64_t(2 * sm_count())));
+    const size_t need = size_t(L.grid) * lanes * nb * 64;
+    if (st.scratch_bytes < need) {
+      if (st.scratch) {
+        RS_CUDA(cudaDeviceSynchronize());
+        cudaFree(st.scratch);
+        st.scratch = nullptr;
+        st.scratch_bytes = 0;
+      }
+      RS_CUDA(cudaMalloc(&st.scratch, need));
+      st.scratch_bytes = need;
+    }
+    L.args.scratch = st.scratch;
+  }
+  return RSGPU_OK;
+}
+
+// Error locators for a presence pattern, built on the GPU (K7a) and kept
+// resident; returns the plan.
+int decode_plan(Codec &c, const uint8_t *present, LeoPlan **out, cudaStream_t s,
+                std::vector<std::pair<std::string, const uint8_t *>> &pending) {
+  LeopardState &st = *c.leo;
+  std::string key(reinterpret_cast<const char *>(present), c.k + c.m);
+  auto it = st.plans.find(key);
+  if (it != st.plans.end()) {
+    *out = &it->second;
+    return RSGPU_OK;
+  }
+  LeoPlan plan;
+  RS_CUDA(cudaMalloc(&plan.err, st.n * 2));
+  plan.input_count = st.m;
+  for (size_t i = 0; i < c.k; ++i)
+    if (present[i]) plan.input_count = uint32_t(st.m + i + 1);
+  auto ins = st.plans.emplace(key, plan);
+  pending.emplace_back(key, present);
+  *out = &ins.first->second;
+  (void)s;
+  return RSGPU_OK;
+}
+
+int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>> &pending, cudaStream_t s) {
+  if (pending.empty()) return RSGPU_OK;
+  LeopardState &st = *c.leo;
+  const size_t total = c.k + c.m;
+  std::vector<uint8_t> pres(pending.size() * total);
+  for (size_t i = 0; i < pending.size(); ++i) std::memcpy(&pres[i * total], pending[i].first.data(), total);
+  uint8_t *d_pres = nullptr;
+  RS_CUDA(cudaMalloc(&d_pres, pres.size()));
+  RS_CUDA(cudaMemcpy(d_pres, pres.data(), pres.size(), cudaMemcpyHostToDevice));
+  std::vector<const uint8_t *> pp(pending.size());
+  std::vector<uint16_t *> oo(pending.size());
+  for (size_t i = 0; i < pending.size(); ++i) {
+    pp[i] = d_pres + i * total;
+    oo[i] = st.plans[pending[i].first].err;
+  }
+  void *d_pp = nullptr, *d_oo = nullptr;
+  RS_CUDA(cudaMalloc(&d_pp, pp.size() * sizeof(void *)));
+  RS_CUDA(cudaMalloc(&d_oo, oo.size() * sizeof(void *)));
+  RS_CUDA(cudaMemcpy(d_pp, pp.data(), pp.size() * sizeof(void *), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMemcpy(d_oo, oo.data(), oo.size() * sizeof(void *), cudaMemcpyHostToDevice));
+  const int bits = st.field->bits;
+  const size_t smem = size_t(1u << bits) * 2;
+  if (bits == 16) {
+    RS_CUDA(cudaFuncSetAttribute(k_leo_locator<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_leo_locator<16><<<int(pending.size()), 1024, smem, s>>>(
+        static_cast<const uint8_t *const *>(d_pp), static_cast<uint16_t *const *>(d_oo), st.field->d_walsh,
+        uint32_t(c.k), uint32_t(c.m), st.m, st.n);
+  } else {
+    k_leo_locator<8><<<int(pending.size()), 256, smem, s>>>(
+        static_cast<const uint8_t *const *>(d_pp), static_cast<uint16_t *const *>(d_oo), st.field->d_walsh,
+        uint32_t(c.k), uint32_t(c.m), st.m, st.n);
+  }
+  launch_counter_add(1);
+  RS_CUDA(cudaGetLastError());
+  RS_CUDA(cudaStreamSynchronize(s));
+  cudaFree(d_pres);
+  cudaFree(d_pp);
+  cudaFree(d_oo);
+  pending.clear();
+  return RSGPU_OK;
+}
+
+int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
+              int goal, const uint8_t *required, size_t n_required, uint32_t *flags, LeoLaunch &L,
+              cudaStream_t s) {
+  LeopardState &st = *c.leo;
+  const size_t total = c.k + c.m;
+  L.codec = &c;
+  L.decode = op == RSGPU_OP_RECONSTRUCT;
+  L.verify = op == RSGPU_OP_VERIFY;
+  std::vector<LeoJob> jobs;
+  std::vector<uint8_t> roles;
+  std::vector<size_t> role_off;
+  {
+    std::lock_guard<std::mutex> g(st.mu);
+    std::vector<std::pair<std::string, const uint8_t *>> pending;
+    for (size_t i = 0; i < n_stripes; ++i) {
+      LeoJob j{};
+      j.ptr_off = uint32_t(i * total);
+      j.flag_idx = uint32_t(i);
+      if (L.decode) {
+        const uint8_t *pr = present + i * total;
+        size_t np = 0;
+        bool any_target = false;
+        const size_t base = roles.size();
+        for (size_t x = 0; x < total; ++x) {
+          np += pr[x] ? 1 : 0;
+          bool want = goal == RSGPU_GOAL_ALL || (goal == RSGPU_GOAL_DATA && x < c.k) ||
+                      (goal == RSGPU_GOAL_REQUIRED && x < n_required && required[x]);
+          uint8_t role = pr[x] ? 1 : (want ? 2 : 0);
+          any_target |= role == 2;
+          roles.push_back(role);
+        }
+        // Missing beyond the parity count cannot be recovered
+        // (src/core/leopard_gf16/decode.rs:744-748).
+        if (total - np > c.m) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+        if (np == total || !any_target) {
+          roles.resize(base);
+          continue;
+        }
+        LeoPlan *plan = nullptr;
+        int rc = decode_plan(c, pr, &plan, s, pending);
+        if (rc) return rc;
+        j.err = plan->err;
+        j.input_count = plan->input_count;
+        role_off.push_back(base);
+      }
+      jobs.push_back(j);
+    }
+    int rc = build_locators(c, pending, s);
+    if (rc) return rc;
+  }
+  // Blob: jobs | pointers | roles.
+  const size_t jb = jobs.size() * sizeof(LeoJob);
+  const size_t pb = n_stripes * total * sizeof(void *);
+  std::vector<uint8_t> blob(jb + pb + roles.size() + 16);
+  std::memcpy(blob.data() + jb, shards, pb);
+  std::memcpy(blob.data() + jb + pb, roles.data(), roles.size());
+  RS_CUDA(cudaMalloc(&L.d_blob, std::max<size_t>(blob.size(), 16)));
+  uint8_t *dbase = static_cast<uint8_t *>(L.d_blob);
+  for (size_t i = 0; i < jobs.size(); ++i)
+    if (L.decode) jobs[i].role = dbase + jb + pb + role_off[i];
+  std::memcpy(blob.data(), jobs.data(), jb);
+  RS_CUDA(cudaMemcpy(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  LeoArgs &a = L.args;
+  a.jobs = reinterpret_cast<const LeoJob *>(dbase);
+  a.ptrs = reinterpret_cast<const uint8_t *const *>(dbase + jb);
+  a.skew = st.field->d_skew;
+  a.bank = st.field->d_bank;
+  a.flags = flags;
+  a.len = len;
+  a.n_jobs = uint32_t(jobs.size());
+  a.k = uint32_t(c.k);
+  a.p = uint32_t(c.m);
+  a.m = st.m;
+  a.n = st.n;
+  a.mtrunc = st.mtrunc;
+  a.last = st.last;
+  a.mod = st.field->host.mod;
+  const uint32_t lanes = L.decode ? st.n : 2 * st.m;
+  const uint32_t nb_guess = pick_nb(lanes, len);
+  const uint64_t tiles = ((len + nb_guess * 64 - 1) / (nb_guess * 64)) * std::max<size_t>(jobs.size(), 1);
+  const bool b16 = st.field->bits == 16;
+  int rc;
+  if (L.decode)
+    rc = b16 ? configure(k_leo_decode<16, false>, L, lanes, len, tiles)
+             : configure(k_leo_decode<8, false>, L, lanes, len, tiles);
+  else if (L.verify)
+    rc = b16 ? configure(k_leo_encode<16, true, false>, L, lanes, len, tiles)
+             : configure(k_leo_encode<8, true, false>, L, lanes, len, tiles);
+  else
+    rc = b16 ? configure(k_leo_encode<16, false, false>, L, lanes, len, tiles)
+             : configure(k_leo_encode<8, false, false>, L, lanes, len, tiles);
+  if (rc) return rc;
+  return RSGPU_OK;
+}
+
+}  // namespace
+
+int leo_launch(const LeoLaunch &L, cudaStream_t s) {
+  if (L.args.n_jobs == 0) return RSGPU_OK;
+  const bool b16 = L.codec->leo->field->bits == 16;
+  const LeoArgs &a = L.args;
+  const dim3 grid(L.grid), block(kLeoThreads);
+#define LEO_GO(KERNEL) KERNEL<<<grid, block, L.smem, s>>>(a)
+  if (L.decode) {
+    if (L.global_work) {
+      if (b16) LEO_GO((k_leo_decode<16, true>)); else LEO_GO((k_leo_decode<8, true>));
+    } else {
+      if (b16) LEO_GO((k_leo_decode<16, false>)); else LEO_GO((k_leo_decode<8, false>));
+    }
+  } else if (L.verify) {
+    if (L.global_work) {
+      if (b16) LEO_GO((k_leo_encode<16, true, true>)); else LEO_GO((k_leo_encode<8, true, true>));
+    } else {
+      if (b16) LEO_GO((k_leo_encode<16, true, false>)); else LEO_GO((k_leo_encode<8, true, false>));
+    }
+  } else {
+    if (L.global_work) {
+      if (b16) LEO_GO((k_leo_encode<16, false, true>)); else LEO_GO((k_leo_encode<8, false, true>));
+    } else {
+      if (b16) LEO_GO((k_leo_encode<16, false, false>)); else LEO_GO((k_leo_encode<8, false, false>));
+    }
+  }
+#undef LEO_GO
+  launch_counter_add(1);
+  return cuda_status(cudaGetLastError());
+}
+
+uint32_t leo_kernel_count(const LeoLaunch &L) { return L.args.n_jobs ? 1 : 0; }
+
+int prepare_other(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
+                  int goal, uint32_t *flags, std::shared_ptr<LeoLaunch> &out) {
+  if (c.family == RSGPU_FAMILY_CLASSIC) return prepare_tower(c, op, n_stripes, shards, present, len, goal, flags, out);
+  auto L = std::make_shared<LeoLaunch>();
+  int rc = build_leo(c, op, n_stripes, shards, present, len, goal, nullptr, 0, flags, *L, nullptr);
+  if (rc) return rc;
+  out = L;
+  return RSGPU_OK;
+}
+
+static int run_once(Codec &c, int op, size_t n, uint8_t *const *shards, const uint8_t *present, size_t len, int goal,
+                    const uint8_t *required, size_t n_required, uint32_t *flags, cudaStream_t s) {
+  LeoLaunch L;
+  int rc = build_leo(c, op, n, shards, present, len, goal, required, n_required, flags, L, s);
+  if (rc) return rc;
+  rc = leo_launch(L, s);
+  if (rc) return rc;
+  // The launch's tables are freed with L; wait for the kernel first.
+  RS_CUDA(cudaStreamSynchronize(s));
+  return RSGPU_OK;
+}
+
+int leopard_encode(Codec &c, size_t n, uint8_t *const *shards, size_t len, cudaStream_t s) {
+  return run_once(c, RSGPU_OP_ENCODE, n, shards, nullptr, len, 0, nullptr, 0, nullptr, s);
+}
+
+int leopard_verify(Codec &c, size_t n, const uint8_t *const *shards, size_t len, uint8_t *ok, cudaStream_t s) {
+  uint32_t *flags = nullptr;
+  RS_CUDA(cudaMalloc(&flags, std::max<size_t>(n, 1) * 4));
+  RS_CUDA(cudaMemsetAsync(flags, 0, std::max<size_t>(n, 1) * 4, s));
+  int rc = run_once(c, RSGPU_OP_VERIFY, n, const_cast<uint8_t *const *>(shards), nullptr, len, 0, nullptr, 0, flags, s);
+  std::vector<uint32_t> f(n);
+  if (rc == RSGPU_OK) {
+    RS_CUDA(cudaMemcpy(f.data(), flags, n * 4, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) ok[i] = f[i] ? 0 : 1;
+  }
+  cudaFree(flags);
+  return rc;
+}
+
+int leopard_reconstruct(Codec &c, size_t n, uint8_t *const *shards, const uint8_t *present, size_t len, int goal,
+                        const uint8_t *required, size_t n_required, cudaStream_t s) {
+  return run_once(c, RSGPU_OP_RECONSTRUCT, n, shards, present, len, goal, required, n_required, nullptr, s);
+}
+
+}  // namespace rsgpu

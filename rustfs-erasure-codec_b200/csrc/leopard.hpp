@@ -18,6 +18,8 @@ struct LeoLaunch;
 int prepare_other(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
                   int goal, uint32_t *flags, std::shared_ptr<LeoLaunch> &out);
 int leo_launch(const LeoLaunch &l, cudaStream_t s);
+int prepare_tower(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
+                  int goal, uint32_t *flags, std::shared_ptr<LeoLaunch> &out);
 uint32_t leo_kernel_count(const LeoLaunch &l);
 
 // src/core/leopard.rs:191-223 (resolve_codec_family) for the byte field.
