@@ -60,6 +60,7 @@ enum {
   RSGPU_ERR_INVALID_ARGUMENT = 102,
   RSGPU_ERR_DEVICE_TIMEOUT = 103,
   RSGPU_ERR_NO_DEVICE = 104,
+  RSGPU_ERR_SCRATCH_LIMIT = 105,
 };
 
 enum { RSGPU_MEM_HOST = 0, RSGPU_MEM_DEVICE = 1 };
@@ -215,6 +216,38 @@ int32_t rsgpu_batch_verify_result(rsgpu_batch *batch, uint8_t *ok, void *stream)
 /* Kernels one launch of this batch issues. */
 uint32_t rsgpu_batch_kernel_count(const rsgpu_batch *batch);
 void rsgpu_batch_free(rsgpu_batch *batch);
+
+/* ------------------------------------------------------------ no-allocation path */
+/* Leopard reconstruction (every missing shard, like rsgpu_reconstruct with
+ * RSGPU_GOAL_ALL and RSGPU_MEM_DEVICE) that allocates no memory at all.  It
+ * has no counterpart in the reference.
+ *
+ * Who needs it: callers that must not allocate device memory while serving,
+ * for example a storage node that reserved the GPU's memory for its shard
+ * buffers at start-up, or a process held to a fixed device-memory quota.
+ * For them a cudaMalloc can fail when the memory is already spoken for, and
+ * it can also synchronize the device, stalling the other streams mid-request.
+ * The regular entry points allocate job tables, decode plans and, for codes
+ * too wide for shared memory, the work rows; this one uses fixed buffers in
+ * static device memory instead (about 16.3 MiB per GPU, held by every GPU that
+ * loads the library until the process exits).
+ *
+ * Limits: the codec must be Leopard (GF(2^8) or GF(2^16)) with at most
+ * RSGPU_NOALLOC_MAX_LANES transform lanes (next power of two of
+ * next_pow2(parity) + data); larger codes get RSGPU_ERR_SCRATCH_LIMIT.
+ * Shard pointers are device pointers.
+ *
+ * Usage rules: the first call on a device looks up the static buffers'
+ * device addresses (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  The work is queued on `stream` and the call returns
+ * without waiting.  Every call shares the same static buffers, which keep the
+ * previous call's contents (each call rewrites everything it reads before
+ * reading it): two calls whose work overlaps on the GPU, for example on two
+ * streams, race and produce garbage. */
+#define RSGPU_NOALLOC_MAX_LANES 16384u
+#define RSGPU_NOALLOC_SCRATCH_BYTES (16u << 20)
+int32_t rsgpu_leopard_reconstruct_noalloc(const rsgpu_codec *codec, uint8_t *const *shards, const size_t *lens,
+                                          const uint8_t *present, size_t n_shards, void *stream);
 
 /* ------------------------------------------------------------ introspection */
 /* src/core/codec.rs:412-414 (reconstruction_cache_stats): device decode-table

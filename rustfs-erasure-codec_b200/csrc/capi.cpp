@@ -584,6 +584,18 @@ int32_t rsgpu_get_cache_stats(const rsgpu_codec *h, rsgpu_cache_stats *out) {
   return RSGPU_OK;
 }
 
+int32_t rsgpu_leopard_reconstruct_noalloc(const rsgpu_codec *hc, uint8_t *const *shards, const size_t *lens,
+                                          const uint8_t *present, size_t n, void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || !shards || !lens || !present) return RSGPU_ERR_INVALID_ARGUMENT;
+  Codec &c = h->c;
+  if (c.family == RSGPU_FAMILY_CLASSIC) return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY;
+  size_t len = 0;
+  int rc = check_reconstruct(c, lens, present, n, RSGPU_GOAL_ALL, nullptr, 0, &len);
+  if (rc || len == 0) return rc;
+  return rsgpu::leopard_reconstruct_noalloc(c, shards, present, len, S(stream));
+}
+
 uint64_t rsgpu_kernel_launch_count(void) { return rsgpu::launch_counter(); }
 
 const char *rsgpu_error_string(int32_t code) {
@@ -610,6 +622,7 @@ const char *rsgpu_error_string(int32_t code) {
     case RSGPU_ERR_INVALID_ARGUMENT: return "invalid argument (null pointer or undersized output)";
     case RSGPU_ERR_DEVICE_TIMEOUT: return "a bounded device wait expired";
     case RSGPU_ERR_NO_DEVICE: return "no CUDA device available";
+    case RSGPU_ERR_SCRATCH_LIMIT: return "the code is wider than the no-allocation entry point's static buffers allow";
     default: return "unknown error";
   }
 }

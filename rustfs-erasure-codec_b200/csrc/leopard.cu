@@ -969,4 +969,160 @@ int leopard_reconstruct(Codec &c, size_t n, uint8_t *const *shards, const uint8_
   return run_once(c, RSGPU_OP_RECONSTRUCT, n, shards, present, len, goal, required, n_required, nullptr, s);
 }
 
+// ====================================================================== no allocation
+// Reconstruction for callers that cannot allocate device memory: the work
+// rows, the pointer table, the presence/role flags, the error locators and the
+// job descriptor live in file-scope static device arrays instead of
+// allocations.  Host code never hands these names to a kernel (in host code
+// they are stand-ins, not device addresses): set-up resolves each one with
+// cudaGetSymbolAddress once per device, with that device current, and the
+// kernels receive the resolved pointers.
+namespace {
+
+constexpr size_t kNaLanes = RSGPU_NOALLOC_MAX_LANES;
+constexpr size_t kNaScratchWords = RSGPU_NOALLOC_SCRATCH_BYTES / 4;
+static_assert(RSGPU_NOALLOC_SCRATCH_BYTES >= kNaLanes * 64, "one CTA at the lane limit must fit");
+
+__device__ __align__(256) uint32_t na_scratch[kNaScratchWords];  // work rows, one region per CTA
+__device__ __align__(256) const uint8_t *na_ptrs[kNaLanes];      // shard pointers (k + p <= lanes)
+__device__ __align__(256) uint8_t na_present[kNaLanes];
+__device__ __align__(256) uint8_t na_role[kNaLanes];
+__device__ __align__(256) uint16_t na_err[kNaLanes];
+__device__ __align__(256) LeoJob na_job;
+__device__ __align__(256) const uint8_t *na_present_ref[1];
+__device__ __align__(256) uint16_t *na_err_ref[1];
+
+struct NaDevice {
+  bool ready = false;
+  uint32_t *scratch = nullptr;
+  const uint8_t **ptrs = nullptr;
+  uint8_t *present = nullptr, *role = nullptr;
+  uint16_t *err = nullptr;
+  LeoJob *job = nullptr;
+  const uint8_t *const *present_ref = nullptr;
+  uint16_t *const *err_ref = nullptr;
+};
+
+constexpr int kNaMaxDevices = 64;
+NaDevice na_dev[kNaMaxDevices];
+std::mutex na_mu;
+// Host-side staging: static arrays, so a call allocates no host memory either.
+// Copies from them are issued from pageable memory, which the driver consumes
+// before cudaMemcpyAsync returns, so the next call may overwrite them at once.
+const uint8_t *na_h_ptrs[kNaLanes];
+uint8_t na_h_present[kNaLanes];
+uint8_t na_h_role[kNaLanes];
+LeoJob na_h_job;
+
+int na_setup(int dev, NaDevice &d) {
+  void *p = nullptr;
+  RS_CUDA(cudaGetSymbolAddress(&p, na_scratch));
+  d.scratch = static_cast<uint32_t *>(p);
+  RS_CUDA(cudaGetSymbolAddress(&p, na_ptrs));
+  d.ptrs = static_cast<const uint8_t **>(p);
+  RS_CUDA(cudaGetSymbolAddress(&p, na_present));
+  d.present = static_cast<uint8_t *>(p);
+  RS_CUDA(cudaGetSymbolAddress(&p, na_role));
+  d.role = static_cast<uint8_t *>(p);
+  RS_CUDA(cudaGetSymbolAddress(&p, na_err));
+  d.err = static_cast<uint16_t *>(p);
+  RS_CUDA(cudaGetSymbolAddress(&p, na_job));
+  d.job = static_cast<LeoJob *>(p);
+  RS_CUDA(cudaGetSymbolAddress(&p, na_present_ref));
+  d.present_ref = static_cast<const uint8_t *const *>(p);
+  RS_CUDA(cudaGetSymbolAddress(&p, na_err_ref));
+  d.err_ref = static_cast<uint16_t *const *>(p);
+  // The locator kernel reads its pattern and output through one-entry
+  // pointer arrays; point them at the static presence and locator arrays.
+  const uint8_t *pres = d.present;
+  uint16_t *err = d.err;
+  RS_CUDA(cudaMemcpy(const_cast<const uint8_t **>(d.present_ref), &pres, sizeof(pres), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMemcpy(const_cast<uint16_t **>(d.err_ref), &err, sizeof(err), cudaMemcpyHostToDevice));
+  (void)dev;
+  d.ready = true;
+  return RSGPU_OK;
+}
+
+}  // namespace
+
+int leopard_reconstruct_noalloc(Codec &c, uint8_t *const *shards, const uint8_t *present, size_t len,
+                                cudaStream_t s) {
+  LeopardState &st = *c.leo;
+  const size_t total = c.k + c.m;
+  if (st.n > kNaLanes || total > kNaLanes) return RSGPU_ERR_SCRATCH_LIMIT;
+  size_t np = 0;
+  for (size_t i = 0; i < total; ++i) np += present[i] ? 1 : 0;
+  if (np == total) return RSGPU_OK;
+  if (total - np > c.m) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+  if (c.device < 0 || c.device >= kNaMaxDevices) return RSGPU_ERR_INVALID_ARGUMENT;
+  int prev = 0;
+  RS_CUDA(cudaGetDevice(&prev));
+  if (prev != c.device) RS_CUDA(cudaSetDevice(c.device));
+  std::lock_guard<std::mutex> g(na_mu);
+  NaDevice &d = na_dev[c.device];
+  int rc = d.ready ? RSGPU_OK : na_setup(c.device, d);
+  if (rc == RSGPU_OK) {
+    uint32_t input_count = st.m;
+    for (size_t i = 0; i < total; ++i) {
+      na_h_ptrs[i] = shards[i];
+      na_h_present[i] = present[i] ? 1 : 0;
+      na_h_role[i] = present[i] ? 1 : 2;
+      if (i < c.k && present[i]) input_count = uint32_t(st.m + i + 1);
+    }
+    na_h_job = LeoJob{};
+    na_h_job.err = d.err;
+    na_h_job.role = d.role;
+    na_h_job.input_count = input_count;
+    cudaError_t e = cudaMemcpyAsync(d.ptrs, na_h_ptrs, total * sizeof(void *), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d.present, na_h_present, total, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d.role, na_h_role, total, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d.job, &na_h_job, sizeof(LeoJob), cudaMemcpyHostToDevice, s);
+    rc = cuda_status(e);
+  }
+  if (rc == RSGPU_OK) {
+    // Error locators for this pattern (K7a) into the static locator array;
+    // every entry the decode reads (indices < n) is rewritten.
+    const int bits = st.field->bits;
+    const size_t lsmem = size_t(1u << bits) * 2;
+    if (bits == 16) {
+      cudaFuncSetAttribute(k_leo_locator<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lsmem));
+      k_leo_locator<16><<<1, 1024, lsmem, s>>>(d.present_ref, d.err_ref, st.field->d_walsh, uint32_t(c.k),
+                                               uint32_t(c.m), st.m, st.n);
+    } else {
+      k_leo_locator<8><<<1, 256, lsmem, s>>>(d.present_ref, d.err_ref, st.field->d_walsh, uint32_t(c.k),
+                                             uint32_t(c.m), st.m, st.n);
+    }
+    LeoArgs a{};
+    a.jobs = d.job;
+    a.ptrs = d.ptrs;
+    a.skew = st.field->d_skew;
+    a.bank = st.field->d_bank;
+    a.scratch = d.scratch;
+    a.len = len;
+    a.n_jobs = 1;
+    a.k = uint32_t(c.k);
+    a.p = uint32_t(c.m);
+    a.m = st.m;
+    a.n = st.n;
+    a.mtrunc = st.mtrunc;
+    a.last = st.last;
+    a.nb = 1;
+    a.lanes = st.n;
+    a.mod = st.field->host.mod;
+    // Every row a CTA reads is written first (step 1 loads or zeroes all n
+    // rows of its region), so the scratch needs no clearing between calls.
+    const uint64_t tiles = len / 64;
+    const uint64_t slots = kNaScratchWords / (uint64_t(st.n) * kRowWords);
+    const int grid = int(std::min<uint64_t>(tiles, std::min<uint64_t>(slots, 4 * 148)));
+    if (bits == 16)
+      k_leo_decode<16, true><<<grid, kLeoThreads, 0, s>>>(a);
+    else
+      k_leo_decode<8, true><<<grid, kLeoThreads, 0, s>>>(a);
+    launch_counter_add(2);
+    rc = cuda_status(cudaGetLastError());
+  }
+  if (prev != c.device) cudaSetDevice(prev);
+  return rc;
+}
+
 }  // namespace rsgpu

@@ -33,6 +33,10 @@ int leopard_verify(Codec &c, size_t n_stripes, const uint8_t *const *shards, siz
 int leopard_reconstruct(Codec &c, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
                         int goal, const uint8_t *required, size_t n_required, cudaStream_t s);
 
+// No-allocation Leopard reconstruction (leopard.cu): static device buffers only.
+int leopard_reconstruct_noalloc(Codec &c, uint8_t *const *shards, const uint8_t *present, size_t len,
+                                cudaStream_t s);
+
 int tower_encode(Codec &c, size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s);
 int tower_verify(Codec &c, size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok,
                  cudaStream_t s);

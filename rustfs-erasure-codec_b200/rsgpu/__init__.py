@@ -29,7 +29,7 @@ ERROR_NAMES = {
     9: "IncorrectShardSize", 10: "TooFewShardsPresent", 11: "EmptyShard", 12: "InvalidShardFlags",
     13: "InvalidIndex", 14: "InvalidCustomMatrix", 15: "UnsupportedCodecFamily",
     16: "UnsupportedLeopardPrototype", 100: "Cuda", 101: "OutOfMemory", 102: "InvalidArgument",
-    103: "DeviceTimeout", 104: "NoDevice",
+    103: "DeviceTimeout", 104: "NoDevice", 105: "ScratchLimit",
 }
 
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -114,6 +114,7 @@ def _lib():
             "rsgpu_batch_verify_result": (I32, [P, U8P, P]),
             "rsgpu_batch_kernel_count": (ctypes.c_uint32, [P]),
             "rsgpu_batch_free": (None, [P]),
+            "rsgpu_leopard_reconstruct_noalloc": (I32, [P, PP, SZP, U8P, SZ, P]),
             "rsgpu_kernel_launch_count": (ctypes.c_uint64, []),
             "rsgpu_error_string": (ctypes.c_char_p, [I32]),
             "rsgpu_version": (ctypes.c_char_p, []),
