@@ -201,6 +201,58 @@ def run_reference(args, rank, world):
     return 0
 
 
+# --------------------------------------------------------------------- profiling cases
+def _case_encode_10x4_64k():
+    """512 stripes x 10+4 x 64 KiB (470 MB per launch, above L2): three encode launches."""
+    import torch
+
+    import rsgpu
+
+    k, m, size, n = 10, 4, 65536, 512
+    codec = rsgpu.ReedSolomon(k, m)
+    buf = torch.randint(0, 256, (n, k + m, size), dtype=torch.uint8, device="cuda")
+    offs = np.arange(n * (k + m), dtype=np.uint64) * np.uint64(size)
+    enc = codec.prepare_batch("encode", rsgpu.device_pointer_table(buf.data_ptr(), offs), size)
+    for _ in range(3):
+        enc.launch()
+    torch.cuda.synchronize()
+    print("case encode-10x4-64k done")
+    return 0
+
+
+def _case_leopard(field, k, m, size, n, op):
+    import torch
+
+    import rsgpu
+
+    fam = "leopard_gf8" if field == 8 else "leopard_gf16"
+    codec = rsgpu.ReedSolomon(k, m, rsgpu.CodecOptions(codec_family=fam))
+    buf = torch.randint(0, 256, (n, k + m, size), dtype=torch.uint8, device="cuda")
+    offs = np.arange(n * (k + m), dtype=np.uint64) * np.uint64(size)
+    ptrs = rsgpu.device_pointer_table(buf.data_ptr(), offs)
+    if op == "encode":
+        b = codec.prepare_batch("encode", ptrs, size)
+    else:
+        rng = np.random.default_rng(SEED)
+        pats = np.ones((n, k + m), np.uint8)
+        for s in range(n):
+            pats[s, rng.choice(k + m, size=m, replace=False)] = 0
+        b = codec.prepare_batch("reconstruct", ptrs, size, present=pats)
+    for _ in range(3):
+        b.launch()
+    torch.cuda.synchronize()
+    print(f"case leopard gf{field} {k}+{m} {op} done")
+    return 0
+
+
+PROFILE_CASES = {
+    "encode-10x4-64k": _case_encode_10x4_64k,
+    "lgf16-decode-1024x512": lambda: _case_leopard(16, 1024, 512, 16384, 16, "decode"),
+    "lgf16-encode-1024x512": lambda: _case_leopard(16, 1024, 512, 16384, 16, "encode"),
+    "lgf8-encode-32x16": lambda: _case_leopard(8, 32, 16, 1 << 20, 16, "encode"),
+}
+
+
 # --------------------------------------------------------------------- GPU side
 def main():
     ap = argparse.ArgumentParser()
@@ -211,7 +263,11 @@ def main():
     ap.add_argument("--stripes", type=int, default=STRIPES)
     ap.add_argument("--e2e-stripes", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--case", default=None, choices=sorted(PROFILE_CASES),
+                    help="run one small profiling case (three launches of one kernel) and exit")
     args = ap.parse_args()
+    if args.case:
+        return PROFILE_CASES[args.case]()
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

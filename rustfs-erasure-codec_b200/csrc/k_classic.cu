@@ -391,7 +391,8 @@ void launch_variant(const ApplyArgs &a, int variant, cudaStream_t s) {
     case 2: launch_vec<1, 2, 4, 2, VERIFY>(a, s); break;
     case 3: launch_vec<1, 1, 8, 1, VERIFY>(a, s); break;
     case 4: launch_vec<1, 1, 4, 1, VERIFY>(a, s); break;
-    default: launch_vec<1, 2, 4, 1, VERIFY>(a, s); break;
+    case 1: launch_vec<1, 2, 4, 1, VERIFY>(a, s); break;
+    default: launch_vec<1, 2, 4, 0, VERIFY>(a, s); break;
   }
 }
 
@@ -400,7 +401,7 @@ void launch_variant(const ApplyArgs &a, int variant, cudaStream_t s) {
 int &apply_variant() {
   static int v = [] {
     const char *e = getenv("RSGPU_APPLY_VARIANT");
-    return e ? atoi(e) : 1;
+    return e ? atoi(e) : 0;
   }();
   return v;
 }
