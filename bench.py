@@ -250,6 +250,9 @@ PROFILE_CASES = {
     "lgf16-decode-1024x512": lambda: _case_leopard(16, 1024, 512, 16384, 16, "decode"),
     "lgf16-encode-1024x512": lambda: _case_leopard(16, 1024, 512, 16384, 16, "encode"),
     "lgf8-encode-32x16": lambda: _case_leopard(8, 32, 16, 1 << 20, 16, "encode"),
+    "lgf8-decode-32x16": lambda: _case_leopard(8, 32, 16, 1 << 20, 16, "decode"),
+    "lgf8-encode-128x64": lambda: _case_leopard(8, 128, 64, 1 << 19, 16, "encode"),
+    "lgf8-decode-128x64": lambda: _case_leopard(8, 128, 64, 1 << 19, 16, "decode"),
 }
 
 

@@ -217,6 +217,149 @@ int32_t rsgpu_batch_verify_result(rsgpu_batch *batch, uint8_t *ok, void *stream)
 uint32_t rsgpu_batch_kernel_count(const rsgpu_batch *batch);
 void rsgpu_batch_free(rsgpu_batch *batch);
 
+/* ------------------------------------------------------------ mixed batches */
+/* A mixed batch runs many stripes of different codecs (classic GF(2^8),
+ * Leopard GF(2^8) / GF(2^16)), shard lengths and operations in ONE persistent
+ * kernel over a device work queue of column tiles, optionally launched
+ * through a captured CUDA graph.  Like a prepared batch it is planned once and
+ * launched any number of times without allocating or synchronizing; shard
+ * pointers are device pointers that must stay valid, and every codec must
+ * outlive the batch.  Each operation gets a plan (algorithm, tile); every plan
+ * writes the same bytes, so the plan only changes the speed.  No reference
+ * counterpart: the reference serves one stripe per call
+ * (src/core/encode.rs:935-972, src/core/reconstruct.rs:731-790,
+ * src/core/verify.rs:14-174), and these batches are the many-call form of
+ * exactly those operations.  Tower-field (galois_16) codecs are not accepted
+ * (RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY). */
+typedef struct rsgpu_mix rsgpu_mix;
+typedef struct rsgpu_mix_op {
+  const rsgpu_codec *codec;
+  int32_t op;              /* RSGPU_OP_* */
+  int32_t goal;            /* reconstruct: RSGPU_GOAL_ALL or RSGPU_GOAL_DATA */
+  uint8_t *const *shards;  /* k + m device pointers */
+  const uint8_t *present;  /* reconstruct: k + m flags (ignored otherwise) */
+  size_t shard_len;
+} rsgpu_mix_op;
+
+/* Algorithms: RSGPU_ALGO_APPLY = the K1 table kernel over the operation's
+ * coefficient matrix (classic; for Leopard GF(2^8) the FFT pipeline written
+ * out as a dense matrix over the Leopard field); tile 0 = 8 KiB of columns and
+ * four outputs per pass over the inputs, 1 = 4 KiB and four, 2 = 4 KiB and
+ * eight.  RSGPU_ALGO_FFT = the Leopard transform, tile
+ * t = 2^t 64-byte column blocks per work item (t = 1..3; transforms of at
+ * most 16 lanes run in registers on 1 KiB of columns whatever t is). */
+enum { RSGPU_ALGO_APPLY = 0, RSGPU_ALGO_FFT = 1 };
+typedef struct rsgpu_plan {
+  int32_t algo;
+  int32_t tile;
+} rsgpu_plan;
+
+/* Planners: FIXED = a fixed rule per family; TABLE = the measured autotuner
+ * table (FIXED where it has no entry); MODEL = the learned cost model, with
+ * the table as its fallback.  Order: SUBMIT keeps the operations' order in the
+ * queue; COST puts the most expensive work items first. */
+enum { RSGPU_PLANNER_FIXED = 0, RSGPU_PLANNER_TABLE = 1, RSGPU_PLANNER_MODEL = 2 };
+enum { RSGPU_ORDER_SUBMIT = 0, RSGPU_ORDER_COST = 1 };
+typedef struct rsgpu_mix_options {
+  int32_t planner;     /* RSGPU_PLANNER_* */
+  int32_t order;       /* RSGPU_ORDER_* */
+  int32_t graph;       /* nonzero: launch through a captured CUDA graph */
+  int32_t ctas_per_sm; /* resident CTAs per SM (0: as many as fit) */
+} rsgpu_mix_options;
+
+typedef struct rsgpu_mix_info {
+  size_t n_ops, n_jobs, n_items, n_classes;
+  uint64_t algorithmic_bytes; /* bytes read + written by one launch */
+  size_t device_bytes;        /* device memory the batch holds */
+  uint32_t grid, smem_bytes, kernels_per_launch, pad;
+} rsgpu_mix_info;
+
+void rsgpu_mix_options_default(rsgpu_mix_options *out);
+int32_t rsgpu_mix_prepare(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_mix_options *opts, rsgpu_mix **out);
+/* As rsgpu_mix_prepare with an explicit plan per operation (the autotuner's
+ * sweep uses it); RSGPU_ERR_INVALID_ARGUMENT for a plan the codec cannot run. */
+int32_t rsgpu_mix_prepare_planned(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *plans,
+                                  const rsgpu_mix_options *opts, rsgpu_mix **out);
+int32_t rsgpu_mix_launch(rsgpu_mix *mix, void *stream);
+/* Wait for `stream`, then write one flag per operation: verify operations 1
+ * when the parity matched, 0 otherwise; other operations 1. */
+int32_t rsgpu_mix_results(rsgpu_mix *mix, uint8_t *ok, void *stream);
+int32_t rsgpu_mix_get_info(const rsgpu_mix *mix, rsgpu_mix_info *out);
+/* The plan chosen for each operation. */
+int32_t rsgpu_mix_get_plans(const rsgpu_mix *mix, rsgpu_plan *out, size_t n_ops);
+void rsgpu_mix_free(rsgpu_mix *mix);
+
+/* ------------------------------------------------------------ autotuner and cost model */
+/* The plan of a mixed-batch operation is chosen from measurements.
+ *
+ * Autotuner: rsgpu_tune measures every valid plan for each distinct class
+ * among `ops` (class = family, k, m, operation, erasure-count bucket,
+ * shard-length bucket), each on synthetic device stripes of the class's own
+ * shape, and keeps the fastest in a process-wide table (the
+ * RSGPU_PLANNER_TABLE planner).  Every measurement is also kept as a sample.
+ *
+ * Cost model: a small MLP (RSGPU_MODEL_FEATURES inputs, two hidden layers of
+ * RSGPU_MODEL_HIDDEN ReLU units, one output per plan: predicted log2 GB/s)
+ * trained and evaluated by the library's own CUDA kernels on the tuner's
+ * samples (the RSGPU_PLANNER_MODEL planner; a class the table has measured
+ * keeps its measured plan).  Plans never change bytes, so neither can change
+ * an output.  Features of an operation (rsgpu_plan_features): classic GF(2^8),
+ * Leopard GF(2^8), Leopard GF(2^16) indicators; log2 k / 16; log2 m / 16;
+ * (log2 shard_len - 12) / 10; encode, reconstruct, verify indicators;
+ * erased / m; erased data shards / max(erased, 1).  Plan order of the model's
+ * outputs (rsgpu_plan_index): APPLY tiles 0, 1, 2, then FFT tiles 1, 2, 3.
+ * No reference counterpart. */
+#define RSGPU_MODEL_FEATURES 11
+#define RSGPU_MODEL_PLANS 6
+#define RSGPU_MODEL_HIDDEN 32
+typedef struct rsgpu_tune_options {
+  size_t target_bytes; /* shard bytes per measured batch (0: 256 MiB) */
+  int32_t repeats;     /* timed launches per plan, best kept (0: 3) */
+  int32_t pad;
+} rsgpu_tune_options;
+typedef struct rsgpu_tune_sample {
+  float features[RSGPU_MODEL_FEATURES];
+  rsgpu_plan plan;
+  float gbps; /* algorithmic bytes / second / 1e9 */
+} rsgpu_tune_sample;
+int32_t rsgpu_plan_features(const rsgpu_mix_op *op, float *out);
+/* Index of `plan` among the model's outputs, or -1. */
+int32_t rsgpu_plan_index(rsgpu_plan plan);
+int32_t rsgpu_tune(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_tune_options *opts, size_t *classes_tuned);
+size_t rsgpu_tuner_samples(rsgpu_tune_sample *out, size_t cap);
+size_t rsgpu_tuner_table_size(void);
+/* Best measured plan of the class `op` belongs to (0), or RSGPU_ERR_INVALID_INDEX. */
+int32_t rsgpu_tuner_lookup(const rsgpu_mix_op *op, rsgpu_plan *out);
+int32_t rsgpu_tuner_save(const char *path);
+int32_t rsgpu_tuner_load(const char *path);
+void rsgpu_tuner_clear(void);
+
+typedef struct rsgpu_train_options {
+  int32_t epochs;   /* full-batch Adam steps (0: 2000) */
+  float lr;         /* (0: 3e-3) */
+  uint64_t seed;    /* weight initialization */
+} rsgpu_train_options;
+/* Parameters: W1 (F x H), b1 (H), W2 (H x H), b2 (H), W3 (H x P), b3 (P),
+ * row-major, in that order. */
+size_t rsgpu_model_param_count(void);
+int32_t rsgpu_model_get_params(float *out, size_t n);
+int32_t rsgpu_model_set_params(const float *in, size_t n);
+/* Train on n rows: features (n x F), targets (n x P, log2 GB/s) and mask
+ * (n x P, 1 where the target was measured).  Loss = mean over masked entries
+ * of the squared error.  Installs the trained model for the planner. */
+int32_t rsgpu_model_train(const float *features, const float *targets, const uint8_t *mask, size_t n,
+                          const rsgpu_train_options *opts, float *final_loss);
+/* The same, on the tuner's samples (best of repeated measurements per class
+ * and plan). */
+int32_t rsgpu_model_train_from_tuner(const rsgpu_train_options *opts, float *final_loss);
+/* Forward pass on the GPU: out = n x P predictions. */
+int32_t rsgpu_model_predict(const float *features, size_t n, float *out);
+/* One forward and backward pass with `params` on the GPU (no update): the
+ * loss and its gradient with respect to every parameter. */
+int32_t rsgpu_model_gradients(const float *params, const float *features, const float *targets, const uint8_t *mask,
+                              size_t n, float *loss, float *grads);
+int32_t rsgpu_model_ready(void);
+
 /* ------------------------------------------------------------ no-allocation path */
 /* Leopard reconstruction (every missing shard, like rsgpu_reconstruct with
  * RSGPU_GOAL_ALL and RSGPU_MEM_DEVICE) that allocates no memory at all.  It

@@ -14,17 +14,12 @@
 #include <vector>
 
 #include "codec.hpp"
+#include "handles.hpp"
 #include "leopard.hpp"
 #include "rsgpu.h"
 
 using rsgpu::Codec;
 
-struct rsgpu_codec {
-  Codec c;
-  // internal streams for host-memory staging
-  cudaStream_t io[2] = {nullptr, nullptr};
-  std::mutex io_mu;
-};
 
 struct rsgpu_batch {
   rsgpu_codec *codec = nullptr;
@@ -33,9 +28,12 @@ struct rsgpu_batch {
   rsgpu::ApplyLaunch apply;                // classic families
   std::shared_ptr<rsgpu::LeoLaunch> leo;   // Leopard families
   uint32_t *flags = nullptr;               // verify flags (device)
+  uint32_t *owned_tables = nullptr;        // private copies of the decode tables
   ~rsgpu_batch() {
+    cudaDeviceSynchronize();  // no queued launch may still read the tables
     apply.release(nullptr);
     if (flags) cudaFree(flags);
+    if (owned_tables) cudaFree(owned_tables);
   }
 };
 
@@ -542,7 +540,7 @@ int32_t rsgpu_batch_prepare(const rsgpu_codec *hc, int32_t op, size_t n_stripes,
     std::vector<rsgpu::JobDesc> jobs;
     std::vector<const uint8_t *> dptrs;
     if (op == RSGPU_OP_RECONSTRUCT) {
-      rc = c.reconstruct_jobs(n_stripes, ptrs, present, goal, nullptr, 0, jobs, dptrs, nullptr);
+      rc = c.reconstruct_jobs(n_stripes, ptrs, present, goal, nullptr, 0, jobs, dptrs, nullptr, &b->owned_tables);
       if (rc == RSGPU_OK) rc = rsgpu::cuda_status(cudaDeviceSynchronize());
     } else {
       rc = c.encode_jobs(n_stripes, ptrs, jobs, dptrs, op == RSGPU_OP_VERIFY);

@@ -287,6 +287,26 @@ int Codec::decode_tables(const std::vector<const ClassicPlan *> &plans, std::vec
   return RSGPU_OK;
 }
 
+int Codec::decode_tables_copy(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
+                              uint32_t **owned, cudaStream_t s) {
+  *owned = nullptr;
+  std::lock_guard<std::mutex> g(mu_);
+  int rc = decode_tables(plans, tbls, s);
+  if (rc) return rc;
+  std::unordered_map<const uint32_t *, size_t> slot;
+  for (const uint32_t *t : tbls)
+    if (t && !slot.count(t)) slot.emplace(t, slot.size());
+  if (slot.empty()) return RSGPU_OK;
+  const size_t words = (pool_->block_bytes() + 3) / 4;
+  RS_CUDA(cudaMalloc(reinterpret_cast<void **>(owned), slot.size() * words * 4));
+  for (auto &kv : slot)
+    RS_CUDA(cudaMemcpyAsync(*owned + kv.second * words, kv.first, words * 4, cudaMemcpyDeviceToDevice, s));
+  RS_CUDA(cudaStreamSynchronize(s));
+  for (auto &t : tbls)
+    if (t) t = *owned + slot[t] * words;
+  return RSGPU_OK;
+}
+
 void Codec::stats(rsgpu_cache_stats *out) {
   std::lock_guard<std::mutex> g(mu_);
   *out = stats_;
@@ -399,18 +419,23 @@ int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len
 
 int Codec::reconstruct_jobs(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, int goal,
                             const uint8_t *required, size_t n_required, std::vector<JobDesc> &jobs,
-                            std::vector<const uint8_t *> &ptrs, cudaStream_t s) {
+                            std::vector<const uint8_t *> &ptrs, cudaStream_t s, uint32_t **owned) {
   const size_t total = k + m;
   std::vector<ClassicPlan> plans(n_stripes);
   for (size_t i = 0; i < n_stripes; ++i) {
     int rc = plan_classic(present + i * total, goal, required, n_required, plans[i]);
     if (rc) return rc;
   }
-  std::lock_guard<std::mutex> g(mu_);
   std::vector<const ClassicPlan *> pp(n_stripes);
   for (size_t i = 0; i < n_stripes; ++i) pp[i] = &plans[i];
   std::vector<const uint32_t *> tbls;
-  int rc = decode_tables(pp, tbls, s);
+  int rc;
+  if (owned) {
+    rc = decode_tables_copy(pp, tbls, owned, s);
+  } else {
+    std::lock_guard<std::mutex> g(mu_);
+    rc = decode_tables(pp, tbls, s);
+  }
   if (rc) return rc;
   jobs.clear();
   ptrs.clear();

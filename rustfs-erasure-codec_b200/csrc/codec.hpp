@@ -131,6 +131,12 @@ class Codec {
   int decode_tables(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
                     cudaStream_t s);
   void stats(rsgpu_cache_stats *out);
+  // decode_tables for callers that keep the tables beyond the cache's
+  // control (prepared and mixed batches): the distinct tables are copied into
+  // one new device allocation (*owned, to be cudaFree'd by the caller) before
+  // the cache lock is released, so a later eviction cannot recycle them.
+  int decode_tables_copy(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
+                         uint32_t **owned, cudaStream_t s);
 
  private:
   std::mutex mu_;
@@ -144,12 +150,13 @@ class Codec {
                 uint32_t *flags_dev, cudaStream_t s);
 
  public:
-  // Job lists for the three classic operations over device pointers.
+  // Job lists for the three classic operations over device pointers.  With
+  // `owned`, the decode tables are private copies (see decode_tables_copy).
   int encode_jobs(size_t n_stripes, uint8_t *const *shards, std::vector<JobDesc> &jobs,
                   std::vector<const uint8_t *> &ptrs, bool verify);
   int reconstruct_jobs(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, int goal,
                        const uint8_t *required, size_t n_required, std::vector<JobDesc> &jobs,
-                       std::vector<const uint8_t *> &ptrs, cudaStream_t s);
+                       std::vector<const uint8_t *> &ptrs, cudaStream_t s, uint32_t **owned = nullptr);
 };
 
 int cuda_status(cudaError_t e);

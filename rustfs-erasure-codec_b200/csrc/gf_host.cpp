@@ -260,7 +260,10 @@ int build_tower_matrix(size_t k, size_t m, std::vector<T16> &out) {
 }
 
 void pack_tables(const uint8_t *rows, size_t n_out, size_t n_in, uint32_t *out) {
-  const Gf8 &f = gf8();
+  pack_tables_with(gf8().mul, rows, n_out, n_in, out);
+}
+
+void pack_tables_with(const uint8_t (*mul)[256], const uint8_t *rows, size_t n_out, size_t n_in, uint32_t *out) {
   const size_t groups = (n_out + 3) / 4;
   for (size_t g = 0; g < groups; ++g)
     for (size_t j = 0; j < n_in; ++j) {
@@ -271,11 +274,11 @@ void pack_tables(const uint8_t *rows, size_t n_out, size_t n_in, uint32_t *out) 
         if (o >= n_out) break;
         const uint8_t c = rows[o * n_in + j];
         for (unsigned n = 0; n < 16; ++n) {
-          t[n] |= uint32_t(f.mul[c][n]) << (8 * r);
-          t[16 + n] |= uint32_t(f.mul[c][n << 4]) << (8 * r);
+          t[n] |= uint32_t(mul[c][n]) << (8 * r);
+          t[16 + n] |= uint32_t(mul[c][n << 4]) << (8 * r);
         }
-        for (unsigned i = 0; i < 32; ++i) t[32 + i] |= uint32_t(f.mul[c][i]) << (8 * r);
-        for (unsigned h = 0; h < 8; ++h) t[64 + 2 * r + (h >> 2)] |= uint32_t(f.mul[c][h << 5]) << (8 * (h & 3));
+        for (unsigned i = 0; i < 32; ++i) t[32 + i] |= uint32_t(mul[c][i]) << (8 * r);
+        for (unsigned h = 0; h < 8; ++h) t[64 + 2 * r + (h >> 2)] |= uint32_t(mul[c][h << 5]) << (8 * (h & 3));
       }
     }
 }

@@ -47,5 +47,7 @@ int build_tower_matrix(size_t k, size_t m, std::vector<T16> &out);
 
 // Nibble tables for the matrix-apply kernel; rows is n_out x n_in.
 void pack_tables(const uint8_t *rows, size_t n_out, size_t n_in, uint32_t *out);
+// The same layout for any GF(2)-linear byte field: mul[c][x] = c * x.
+void pack_tables_with(const uint8_t (*mul)[256], const uint8_t *rows, size_t n_out, size_t n_in, uint32_t *out);
 
 }  // namespace rsgpu

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -32,6 +33,8 @@
 #include <vector>
 
 #include "codec.hpp"
+#include "leo_fft.cuh"
+#include "leo_tile.cuh"
 #include "leopard.hpp"
 
 namespace rsgpu {
@@ -141,7 +144,8 @@ struct LeoField {
   LeoTables host;
   uint16_t *d_skew = nullptr;
   uint16_t *d_walsh = nullptr;
-  uint32_t *d_bank = nullptr;  // multiplier tables indexed by log value
+  uint32_t *d_bank = nullptr;   // multiplier tables indexed by log value (half-warp layer kernels)
+  uint32_t *d_kbank = nullptr;  // tables of the register-stage kernels (GF(2^8): 5+3 split; GF(2^16): d_bank)
   explicit LeoField(int b) : bits(b), host(b) {}
 };
 
@@ -174,6 +178,20 @@ static int leo_field(int bits, LeoField **out) {
       }
     RS_CUDA(cudaMalloc(&f->d_bank, bank.size() * 4));
     RS_CUDA(cudaMemcpy(f->d_bank, bank.data(), bank.size() * 4, cudaMemcpyHostToDevice));
+    if (bits == 8) {
+      // Per log value: c * i (i < 32) replicated into four bytes, then the
+      // eight bytes c * (h << 5) packed into two words (layout of leo_fft.cuh).
+      std::vector<uint32_t> kb(size_t(t.order) * kWBank8, 0);
+      for (uint32_t lm = 0; lm < t.order; ++lm) {
+        uint32_t *e = &kb[size_t(lm) * kWBank8];
+        for (uint32_t i = 0; i < 32; ++i) e[i] = uint32_t(t.mul_log(uint16_t(i), uint16_t(lm))) * 0x01010101u;
+        for (uint32_t h = 0; h < 8; ++h) e[32 + (h >> 2)] |= uint32_t(t.mul_log(uint16_t(h << 5), uint16_t(lm))) << (8 * (h & 3));
+      }
+      RS_CUDA(cudaMalloc(&f->d_kbank, kb.size() * 4));
+      RS_CUDA(cudaMemcpy(f->d_kbank, kb.data(), kb.size() * 4, cudaMemcpyHostToDevice));
+    } else {
+      f->d_kbank = f->d_bank;
+    }
     fields[slot] = f;
   }
   *out = fields[slot];
@@ -184,271 +202,11 @@ static int leo_field(int bits, LeoField **out) {
 namespace {
 
 constexpr int kLeoThreads = 512;
-constexpr int kHalfWarps = kLeoThreads / 16;
-constexpr int kRowWords = 16;  // one 64-byte block per lane row
-
-struct LeoJob {
-  uint32_t ptr_off;    // into the pointer table: k + p shard pointers
-  uint32_t flag_idx;   // verify flag
-  const uint16_t *err; // decode: error locators (n entries)
-  const uint8_t *role; // decode: per shard 0 absent, 1 present (input), 2 target (output)
-  uint32_t input_count;
-  uint32_t pad;
-};
-
-struct LeoArgs {
-  const LeoJob *jobs;
-  const uint8_t *const *ptrs;
-  const uint16_t *skew;
-  const uint32_t *bank;
-  uint32_t *flags;
-  uint32_t *scratch;  // global work rows when the lanes do not fit on chip
-  uint64_t len;       // bytes per shard (multiple of 64)
-  uint32_t n_jobs;
-  uint32_t k, p, m, n;  // n: decode lanes (pow2 >= m + k)
-  uint32_t mtrunc, last;
-  uint32_t nb;        // 64-byte column blocks per tile
-  uint32_t lanes;     // rows per tile (encode 2m, decode n)
-  uint32_t mod;
-};
-
-template <int BITS>
-struct Tab;
-template <>
-struct Tab<8> {
-  uint32_t lo, hi;
-};
-template <>
-struct Tab<16> {
-  uint32_t t0, t1, t2, t3;
-};
-
-__device__ __forceinline__ uint32_t shfl16(uint32_t v, uint32_t idx) {
-  uint32_t r;
-  asm("shfl.sync.idx.b32 %0, %1, %2, 0x101f, -1;" : "=r"(r) : "r"(v), "r"(idx));
-  return r;
-}
-
-template <int BITS>
-__device__ __forceinline__ Tab<BITS> load_tab(const uint32_t *bank, uint32_t lm, uint32_t hl);
-template <>
-__device__ __forceinline__ Tab<8> load_tab<8>(const uint32_t *bank, uint32_t lm, uint32_t hl) {
-  const uint2 v = __ldg(reinterpret_cast<const uint2 *>(bank) + lm * 16 + hl);
-  return Tab<8>{v.x, v.y};
-}
-template <>
-__device__ __forceinline__ Tab<16> load_tab<16>(const uint32_t *bank, uint32_t lm, uint32_t hl) {
-  const uint4 v = __ldg(reinterpret_cast<const uint4 *>(bank) + lm * 16 + hl);
-  return Tab<16>{v.x, v.y, v.z, v.w};
-}
-
-// Products of the elements of word w with the half-warp's constant.
-__device__ __forceinline__ uint32_t mulw(uint32_t w, const Tab<8> &t) {
-  const uint32_t s0 = shfl16(t.lo, w) ^ shfl16(t.hi, w >> 4);
-  const uint32_t s1 = shfl16(t.lo, w >> 8) ^ shfl16(t.hi, w >> 12);
-  const uint32_t s2 = shfl16(t.lo, w >> 16) ^ shfl16(t.hi, w >> 20);
-  const uint32_t s3 = shfl16(t.lo, w >> 24) ^ shfl16(t.hi, w >> 28);
-  return __byte_perm(__byte_perm(s0, s1, 0x0040), __byte_perm(s2, s3, 0x4000), 0x7610);
-}
-__device__ __forceinline__ uint32_t mulw(uint32_t w, const Tab<16> &t) {
-  const uint32_t a = shfl16(t.t0, w) ^ shfl16(t.t1, w >> 4) ^ shfl16(t.t2, w >> 8) ^ shfl16(t.t3, w >> 12);
-  const uint32_t b = shfl16(t.t0, w >> 16) ^ shfl16(t.t1, w >> 20) ^ shfl16(t.t2, w >> 24) ^ shfl16(t.t3, w >> 28);
-  return __byte_perm(a, b, 0x7610);
-}
-
-// Split-layout conversion of a 64-byte GF(2^16) block held as 16 words by a
-// half-warp (word t = bytes 4t..4t+3 of the block).
-__device__ __forceinline__ uint32_t user_to_work16(uint32_t w, uint32_t hl) {
-  const uint32_t other = __shfl_xor_sync(0xffffffffu, w, 8, 16);
-  return hl < 8 ? __byte_perm(w, other, 0x5140) : __byte_perm(other, w, 0x7362);
-}
-__device__ __forceinline__ uint32_t work_to_user16(uint32_t w, uint32_t hl) {
-  const uint32_t other = __shfl_xor_sync(0xffffffffu, w, 8, 16);
-  return hl < 8 ? __byte_perm(w, other, 0x6420) : __byte_perm(other, w, 0x7531);
-}
-
-template <int BITS>
-__device__ __forceinline__ uint32_t from_user(uint32_t w, uint32_t hl) {
-  return BITS == 16 ? user_to_work16(w, hl) : w;
-}
-template <int BITS>
-__device__ __forceinline__ uint32_t to_user(uint32_t w, uint32_t hl) {
-  return BITS == 16 ? work_to_user16(w, hl) : w;
-}
-
-// Row r, column block cb: 16 words.
-__device__ __forceinline__ uint32_t *row_ptr(uint32_t *W, uint32_t nb, uint32_t r, uint32_t cb) {
-  return W + (size_t(r) * nb + cb) * kRowWords;
-}
-
-// dit2 on rows x, y of column block cb (forward: x ^= y*c, y ^= x;
-// inverse: y ^= x, x ^= y*c; log_m == mod means only y ^= x).  Both
-// half-warps always execute the shuffles; `valid` gates the stores.
-template <int BITS, bool FWD>
-__device__ __forceinline__ void dit2(uint32_t *W, uint32_t nb, uint32_t cb, uint32_t x, uint32_t y, uint32_t lm,
-                                     const Tab<BITS> &t, uint32_t mod, bool valid, uint32_t hl) {
-  uint32_t *px = row_ptr(W, nb, valid ? x : 0, cb) + hl;
-  uint32_t *py = row_ptr(W, nb, valid ? y : 0, cb) + hl;
-  uint32_t xv = *px, yv = *py;
-  const bool skip = lm == mod;
-  if (FWD) {
-    const uint32_t prod = mulw(yv, t);
-    if (!skip) xv ^= prod;
-    yv ^= xv;
-  } else {
-    yv ^= xv;
-    const uint32_t prod = mulw(yv, t);
-    if (!skip) xv ^= prod;
-  }
-  if (valid) {
-    *px = xv;
-    *py = yv;
-  }
-}
-
-// One radix-4 layer over lanes [0, nl): blocks r < mtrunc step 4*dist, each
-// spanning lanes i, i+dist, i+2dist, i+3dist for i in [r, r+dist).
-// Skew factors: sk[iend + adj], sk[iend + dist + adj], sk[iend + 2dist + adj].
-template <int BITS, bool FWD>
-__device__ void layer4(uint32_t *W, const LeoArgs &a, const uint16_t *sk, int adj, uint32_t nl, uint32_t mtrunc,
-                       uint32_t dist) {
-  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
-  const uint32_t dist4 = dist * 4;
-  const uint32_t nblk = (mtrunc + dist4 - 1) / dist4;
-  const uint32_t items = nblk * dist * a.nb;
-  const uint32_t rounds = (items + kHalfWarps - 1) / kHalfWarps;
-  for (uint32_t rd = 0; rd < rounds; ++rd) {
-    const uint32_t q = rd * kHalfWarps + hw;
-    const bool valid = q < items;
-    const uint32_t qq = valid ? q : 0;
-    const uint32_t cb = qq % a.nb, bq = qq / a.nb;
-    const uint32_t r = (bq / dist) * dist4, i = r + bq % dist;
-    const uint32_t iend = r + dist;
-    const uint32_t m01 = sk[int(iend) + adj], m02 = sk[int(iend + dist) + adj], m23 = sk[int(iend + 2 * dist) + adj];
-    const Tab<BITS> t01 = load_tab<BITS>(a.bank, m01, hl);
-    const Tab<BITS> t23 = load_tab<BITS>(a.bank, m23, hl);
-    const Tab<BITS> t02 = load_tab<BITS>(a.bank, m02, hl);
-    const uint32_t ia = i, ib = i + dist, ic = i + 2 * dist, id = i + 3 * dist;
-    const bool ha = ia < nl, hb = ib < nl, hc = ic < nl, hd = id < nl;
-    if (FWD) {
-      dit2<BITS, true>(W, a.nb, cb, ia, ic, m02, t02, a.mod, valid && ha && hc, hl);
-      dit2<BITS, true>(W, a.nb, cb, ib, id, m02, t02, a.mod, valid && hb && hd, hl);
-      dit2<BITS, true>(W, a.nb, cb, ia, ib, m01, t01, a.mod, valid && ha && hb, hl);
-      dit2<BITS, true>(W, a.nb, cb, ic, id, m23, t23, a.mod, valid && hc && hd, hl);
-    } else {
-      dit2<BITS, false>(W, a.nb, cb, ia, ib, m01, t01, a.mod, valid && ha && hb, hl);
-      dit2<BITS, false>(W, a.nb, cb, ic, id, m23, t23, a.mod, valid && hc && hd, hl);
-      dit2<BITS, false>(W, a.nb, cb, ia, ic, m02, t02, a.mod, valid && ha && hc, hl);
-      dit2<BITS, false>(W, a.nb, cb, ib, id, m02, t02, a.mod, valid && hb && hd, hl);
-    }
-  }
-}
-
-// Final radix-2 layer: pairs (i, i + dist) for i in [0, count), constant per pair.
-template <int BITS, bool FWD>
-__device__ void layer2(uint32_t *W, const LeoArgs &a, uint32_t nl, uint32_t count, uint32_t dist, uint32_t stride,
-                       const uint16_t *lm_of, int lm_fixed) {
-  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
-  const uint32_t items = count * a.nb;
-  const uint32_t rounds = (items + kHalfWarps - 1) / kHalfWarps;
-  for (uint32_t rd = 0; rd < rounds; ++rd) {
-    const uint32_t q = rd * kHalfWarps + hw;
-    const bool valid = q < items;
-    const uint32_t qq = valid ? q : 0;
-    const uint32_t cb = qq % a.nb, i = (qq / a.nb) * stride;
-    const uint32_t lm = lm_fixed >= 0 ? uint32_t(lm_fixed) : lm_of[i];
-    const Tab<BITS> t = load_tab<BITS>(a.bank, lm, hl);
-    dit2<BITS, FWD>(W, a.nb, cb, i, i + dist, lm, t, a.mod, valid && i + dist < nl, hl);
-  }
-}
-
-// Encoder IFFT (src/core/leopard_gf16/mod.rs build_ifft_dit16_plan): lanes >=
-// mtrunc hold zeros, skew base = fft_skew + (m - 1) + group offset.
-template <int BITS>
-__device__ void ifft_encoder(uint32_t *W, const LeoArgs &a, const uint16_t *sk, uint32_t mtrunc) {
-  const uint32_t m = a.m;
-  uint32_t dist = 1, dist4 = 4;
-  while (dist4 <= m) {
-    layer4<BITS, false>(W, a, sk, 0, m, mtrunc, dist);
-    __syncthreads();
-    dist = dist4;
-    dist4 <<= 2;
-  }
-  if (dist < m) {
-    layer2<BITS, false>(W, a, m, dist, dist, 1, nullptr, sk[dist]);
-    __syncthreads();
-  }
-}
-
-// FFT (build_fft_dit16_plan): skew = fft_skew, i_end - 1 indexing.
-template <int BITS>
-__device__ void fft(uint32_t *W, const LeoArgs &a, uint32_t nl, uint32_t mtrunc, uint32_t msize) {
-  uint32_t dist4 = msize, dist = msize >> 2;
-  while (dist != 0) {
-    layer4<BITS, true>(W, a, a.skew, -1, nl, mtrunc, dist);
-    __syncthreads();
-    dist4 = dist;
-    dist >>= 2;
-  }
-  if (dist4 == 2) {
-    layer2<BITS, true>(W, a, nl, (mtrunc + 1) / 2, 1, 2, a.skew, -1);
-    __syncthreads();
-  }
-}
-
-// Decoder IFFT (build_ifft_decode_dit16_plan): blocks r < input_count.
-template <int BITS>
-__device__ void ifft_decoder(uint32_t *W, const LeoArgs &a, uint32_t mtrunc) {
-  const uint32_t n = a.n;
-  uint32_t dist = 1, dist4 = 4;
-  while (dist4 <= n) {
-    layer4<BITS, false>(W, a, a.skew, -1, n, mtrunc, dist);
-    __syncthreads();
-    dist = dist4;
-    dist4 <<= 2;
-  }
-  if (dist < n) {
-    layer2<BITS, false>(W, a, n, dist, dist, 1, nullptr, a.skew[dist - 1]);
-    __syncthreads();
-  }
-}
-
-// Formal derivative (decode.rs compute_formal_derivative16): lane l gains the
-// XOR of lanes l + 2^t for every zero bit t of l with l + 2^t < n.  Lanes
-// are rewritten in increasing order in rounds, so every read sees the value
-// from before the pass.
-__device__ void derivative(uint32_t *W, const LeoArgs &a) {
-  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
-  const uint32_t items = a.n * a.nb;
-  for (uint32_t base = 0; base < items; base += kHalfWarps) {
-    const uint32_t q = base + hw;
-    uint32_t v = 0;
-    const bool valid = q < items;
-    uint32_t l = 0, cb = 0;
-    if (valid) {
-      l = q / a.nb;
-      cb = q % a.nb;
-      v = row_ptr(W, a.nb, l, cb)[hl];
-      for (uint32_t w = 1; l + w < a.n; w <<= 1)
-        if (!(l & w)) v ^= row_ptr(W, a.nb, l + w, cb)[hl];
-    }
-    __syncthreads();
-    if (valid) row_ptr(W, a.nb, l, cb)[hl] = v;
-    __syncthreads();
-  }
-}
-
-__device__ __forceinline__ uint32_t ld_u32(const uint8_t *p) {
-  return __ldg(reinterpret_cast<const uint32_t *>(p));
-}
 
 template <int BITS, bool VERIFY, bool GLOBAL_WORK>
 __global__ void __launch_bounds__(kLeoThreads) k_leo_encode(LeoArgs a) {
   extern __shared__ uint32_t smem[];
   uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
-  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
-  const uint32_t m = a.m;
-  uint32_t *acc = W, *tmp = W + size_t(m) * a.nb * kRowWords;
   const uint64_t tile_bytes = uint64_t(a.nb) * 64;
   const uint32_t tiles_per_job = uint32_t((a.len + tile_bytes - 1) / tile_bytes);
   const uint32_t total = tiles_per_job * a.n_jobs;
@@ -457,55 +215,47 @@ __global__ void __launch_bounds__(kLeoThreads) k_leo_encode(LeoArgs a) {
     const uint32_t job = t / tiles_per_job;
     const uint64_t col0 = uint64_t(t - job * tiles_per_job) * tile_bytes;
     const LeoJob jd = a.jobs[job];
-    const uint8_t *const *ptr = a.ptrs + jd.ptr_off;
-    if (threadIdx.x == 0) bad = 0;
-    // Each group of m data shards passes through an IFFT and is XORed into acc.
-    for (uint32_t g = 0; g * m < a.k; ++g) {
-      uint32_t *dst = g == 0 ? acc : tmp;
-      const uint32_t cnt = g == 0 ? a.mtrunc : (a.k - g * m < m ? a.k - g * m : m);
-      // Rounds keep both halves of every warp in step (the layout shuffle
-      // needs all 32 lanes).
-      for (uint32_t base = 0; base < m * a.nb; base += kHalfWarps) {
-        const uint32_t q = base + hw;
-        const bool valid = q < m * a.nb;
-        const uint32_t l = valid ? q / a.nb : 0, cb = valid ? q % a.nb : 0;
-        const uint64_t col = col0 + uint64_t(cb) * 64;
-        uint32_t v = 0;
-        if (valid && l < cnt && col < a.len) v = ld_u32(ptr[g * m + l] + col + hl * 4);
-        v = from_user<BITS>(v, hl);
-        if (valid) row_ptr(dst, a.nb, l, cb)[hl] = v;
-      }
-      __syncthreads();
-      const uint16_t *sk = a.skew + (m - 1) + g * m;
-      ifft_encoder<BITS>(dst, a, sk, cnt);
-      if (g > 0) {
-        for (uint32_t i = threadIdx.x; i < m * a.nb * kRowWords; i += kLeoThreads) acc[i] ^= tmp[i];
-        __syncthreads();
-      }
-    }
-    fft<BITS>(acc, a, m, a.p, m);
-    // Parity lanes 0..p back to user layout (or compared against the stored parity).
-    uint32_t mismatch = 0;
-    for (uint32_t base = 0; base < a.p * a.nb; base += kHalfWarps) {
-      const uint32_t q = base + hw;
-      const bool valid = q < a.p * a.nb;
-      const uint32_t l = valid ? q / a.nb : 0, cb = valid ? q % a.nb : 0;
-      const uint64_t col = col0 + uint64_t(cb) * 64;
-      const uint32_t v = to_user<BITS>(row_ptr(acc, a.nb, l, cb)[hl], hl);
-      if (valid && col < a.len) {
-        uint32_t *out = reinterpret_cast<uint32_t *>(const_cast<uint8_t *>(ptr[a.k + l]) + col) + hl;
-        if (VERIFY)
-          mismatch |= (*out != v);
-        else
-          *out = v;
-      }
-    }
-    if (VERIFY) {
-      if (mismatch) atomicOr(&bad, 1u);
-      __syncthreads();
-      if (threadIdx.x == 0 && bad) atomicOr(a.flags + jd.flag_idx, 1u);
-    }
-    __syncthreads();
+    leo_encode_tile<BITS, VERIFY, kLeoThreads>(W, a, jd, col0, a.len, &bad);
+  }
+}
+
+constexpr int kFftThreads = 256;
+
+// Register-stage kernels (leo_fft.cuh).  Tile: 4 * kFftThreads bytes when the
+// transform fits in registers (m or n <= 16), else 64 * nb bytes with the
+// work rows in shared memory (or a per-CTA slab of global memory).
+__host__ __device__ inline uint64_t fft_tile_bytes(uint32_t lanes_one_thread, uint32_t nb) {
+  return lanes_one_thread <= 16 ? uint64_t(4 * kFftThreads) : uint64_t(64) * nb;
+}
+
+template <int BITS, bool VERIFY, bool GLOBAL_WORK>
+__global__ void __launch_bounds__(kFftThreads, 2) k_fft_encode(LeoArgs a) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ uint32_t bad;
+  uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
+  const uint64_t tile_bytes = fft_tile_bytes(a.m, a.nb);
+  const uint32_t tiles_per_job = uint32_t((a.len + tile_bytes - 1) / tile_bytes);
+  const uint32_t total = tiles_per_job * a.n_jobs;
+  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+    const uint32_t job = t / tiles_per_job;
+    const uint64_t col0 = uint64_t(t - job * tiles_per_job) * tile_bytes;
+    const LeoJob jd = a.jobs[job];
+    fft_encode_tile<BITS, VERIFY, kFftThreads>(W, a, jd, col0, a.len, &bad);
+  }
+}
+
+template <int BITS, bool GLOBAL_WORK>
+__global__ void __launch_bounds__(kFftThreads, 2) k_fft_decode(LeoArgs a) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
+  const uint64_t tile_bytes = fft_tile_bytes(a.n, a.nb);
+  const uint32_t tiles_per_job = uint32_t((a.len + tile_bytes - 1) / tile_bytes);
+  const uint32_t total = tiles_per_job * a.n_jobs;
+  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+    const uint32_t job = t / tiles_per_job;
+    const uint64_t col0 = uint64_t(t - job * tiles_per_job) * tile_bytes;
+    const LeoJob jd = a.jobs[job];
+    fft_decode_tile<BITS, kFftThreads>(W, a, jd, col0, a.len);
   }
 }
 
@@ -513,8 +263,6 @@ template <int BITS, bool GLOBAL_WORK>
 __global__ void __launch_bounds__(kLeoThreads) k_leo_decode(LeoArgs a) {
   extern __shared__ uint32_t smem[];
   uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
-  const uint32_t hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
-  const uint32_t m = a.m, n = a.n, k = a.k, p = a.p;
   const uint64_t tile_bytes = uint64_t(a.nb) * 64;
   const uint32_t tiles_per_job = uint32_t((a.len + tile_bytes - 1) / tile_bytes);
   const uint32_t total = tiles_per_job * a.n_jobs;
@@ -522,49 +270,7 @@ __global__ void __launch_bounds__(kLeoThreads) k_leo_decode(LeoArgs a) {
     const uint32_t job = t / tiles_per_job;
     const uint64_t col0 = uint64_t(t - job * tiles_per_job) * tile_bytes;
     const LeoJob jd = a.jobs[job];
-    const uint8_t *const *ptr = a.ptrs + jd.ptr_off;
-    // Step 1: lanes 0..p parity, m..m+k data; present lanes scaled by their
-    // error locator, everything else zero.
-    for (uint32_t base = 0; base < n * a.nb; base += kHalfWarps) {
-      const uint32_t q = base + hw;
-      const bool valid = q < n * a.nb;
-      const uint32_t l = valid ? q / a.nb : 0, cb = valid ? q % a.nb : 0;
-      const uint64_t col = col0 + uint64_t(cb) * 64;
-      int shard = -1;
-      if (l < p)
-        shard = int(k + l);
-      else if (l >= m && l < m + k)
-        shard = int(l - m);
-      const bool load = valid && shard >= 0 && jd.role[shard] == 1 && col < a.len;
-      uint32_t v = 0;
-      if (load) v = ld_u32(ptr[shard] + col + hl * 4);
-      // Every half-warp converts and multiplies (shuffles must stay
-      // converged); unused rows multiply zero by the identity.
-      v = from_user<BITS>(v, hl);
-      const uint32_t lm = load ? jd.err[l] : a.mod;
-      const Tab<BITS> tb = load_tab<BITS>(a.bank, lm, hl);
-      v = mulw(v, tb);
-      if (valid) row_ptr(W, a.nb, l, cb)[hl] = v;
-    }
-    __syncthreads();
-    ifft_decoder<BITS>(W, a, jd.input_count);
-    derivative(W, a);
-    fft<BITS>(W, a, n, m + k, n);
-    // Step 5: each target scaled by mod - err and written in user layout.
-    for (uint32_t base = 0; base < (k + p) * a.nb; base += kHalfWarps) {
-      const uint32_t q = base + hw;
-      const bool valid = q < (k + p) * a.nb;
-      const uint32_t i = valid ? q / a.nb : 0, cb = valid ? q % a.nb : 0;
-      const uint64_t col = col0 + uint64_t(cb) * 64;
-      const bool target = valid && jd.role[i] == 2;
-      const uint32_t lane = i >= k ? i - k : m + i;
-      const uint32_t lm = target ? (a.mod - jd.err[lane]) : a.mod;
-      const Tab<BITS> tb = load_tab<BITS>(a.bank, lm, hl);
-      const uint32_t v = to_user<BITS>(mulw(row_ptr(W, a.nb, lane, cb)[hl], tb), hl);
-      if (target && col < a.len)
-        reinterpret_cast<uint32_t *>(const_cast<uint8_t *>(ptr[i]) + col)[hl] = v;
-    }
-    __syncthreads();
+    leo_decode_tile<BITS, kLeoThreads>(W, a, jd, col0, a.len);
   }
 }
 
@@ -638,6 +344,7 @@ struct LeopardState {
   std::vector<void *> owned;
   uint32_t *scratch = nullptr;  // global work rows for the decode of very wide codes
   size_t scratch_bytes = 0;
+  std::vector<uint8_t> dense_enc;  // GF(2^8): the encode map as an m x k matrix
   ~LeopardState() {
     cudaDeviceSynchronize();
     for (auto &kv : plans) cudaFree(kv.second.err);
@@ -648,6 +355,7 @@ struct LeopardState {
 struct LeoLaunch {
   Codec *codec = nullptr;
   bool decode = false, verify = false;
+  int engine = 1;  // 1: register-stage kernels, 0: half-warp layer kernels
   LeoArgs args{};
   void *d_blob = nullptr;  // jobs | pointers | roles
   int grid = 0;
@@ -694,6 +402,134 @@ int sm_count() {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   }
   return sms;
+}
+
+int ilog2(uint32_t v) {
+  int b = 0;
+  while ((1u << b) < v) ++b;
+  return b;
+}
+
+uint8_t stage_byte(int lg, int lgdm) { return uint8_t(lg | (lgdm << 3)); }
+
+// At most four stages: 16 bits of lanes (GF(2^16)) in four-bit stages.
+constexpr int kMaxStages = 4;
+
+// Stage plans of the register-stage kernels (leo_fft.cuh).  IFFT: radix-4
+// layers from distance 1 up, then a radix-2 layer when log2 L is odd; two
+// radix-4 layers per 16-lane stage.  FFT: radix-4 layers from the top down,
+// then the distance-1 radix-2 layer when log2 L is odd.
+int ifft_stages(uint32_t L, uint8_t *out) {
+  const int b = ilog2(L);
+  int used = 0, n = 0;
+  while (b - used >= 4 && n < kMaxStages) {
+    out[n++] = stage_byte(4, used);
+    used += 4;
+  }
+  if (b - used > 0 && n < kMaxStages) out[n++] = stage_byte(b - used, used);
+  return n;
+}
+
+int fft_stages(uint32_t L, uint8_t *out) {
+  const int b = ilog2(L);
+  int n = 0;
+  if (b == 0) return 0;
+  const bool odd = b & 1;
+  int cur = b;
+  const int floor_bits = odd ? 3 : 0;
+  if (b == 1) {
+    out[n++] = stage_byte(1, 0);
+    return n;
+  }
+  if (((cur - floor_bits) % 4) == 2) {
+    out[n++] = stage_byte(2, cur - 2);
+    cur -= 2;
+  }
+  while (cur - floor_bits >= 4 && n < kMaxStages) {
+    out[n++] = stage_byte(4, cur - 4);
+    cur -= 4;
+  }
+  if (odd && n < kMaxStages) out[n++] = stage_byte(3, 0);
+  return n;
+}
+
+uint32_t pack_stages(const uint8_t *st) {
+  return uint32_t(st[0]) | uint32_t(st[1]) << 8 | uint32_t(st[2]) << 16 | uint32_t(st[3]) << 24;
+}
+
+void fill_stages(LeoArgs &a) {
+  uint8_t st[kMaxStages] = {0, 0, 0, 0};
+  a.n_ienc = uint32_t(ifft_stages(a.m, st));
+  a.st_ienc = pack_stages(st);
+  std::memset(st, 0, sizeof(st));
+  a.n_fenc = uint32_t(fft_stages(a.m, st));
+  a.st_fenc = pack_stages(st);
+  std::memset(st, 0, sizeof(st));
+  a.n_idec = uint32_t(ifft_stages(a.n, st));
+  a.st_idec = pack_stages(st);
+  std::memset(st, 0, sizeof(st));
+  a.n_fdec = uint32_t(fft_stages(a.n, st));
+  a.st_fdec = pack_stages(st);
+}
+
+}  // namespace
+
+// Which Leopard kernels run: 1 = register-stage kernels (leo_fft.cuh, the
+// default), 0 = the half-warp layer kernels (leo_tile.cuh).  Both write the
+// same bytes; RSGPU_LEO_ENGINE overrides, and the mixed-batch planner may
+// pick either per operation.
+int &leo_engine() {
+  static int v = [] {
+    const char *e = getenv("RSGPU_LEO_ENGINE");
+    return e ? atoi(e) : 1;
+  }();
+  return v;
+}
+
+namespace {
+
+constexpr size_t kFftSmemBudget = 96 * 1024;  // two resident CTAs per SM
+
+// Work rows and tile width of a register-stage launch: `rows` rows of work
+// (encoder 2m, decoder n) when the transform needs shared memory, i.e. when
+// `reg_lanes` (m or n) exceeds 16.
+template <class K>
+int configure_fft(const K kernel, LeoLaunch &L, uint32_t rows, uint32_t reg_lanes, size_t len, size_t n_jobs) {
+  LeopardState &st = *L.codec->leo;
+  L.args.lanes = rows;
+  size_t smem = 0;
+  uint32_t nb = 2;
+  if (reg_lanes > 16) {
+    while (nb < 8 && size_t(rows) * (nb * 2) * 64 <= kFftSmemBudget && size_t(nb * 2) * 64 <= len) nb *= 2;
+    smem = size_t(rows) * nb * 64;
+  }
+  L.args.nb = nb;
+  L.global_work = smem > 200 * 1024;
+  const uint64_t tile = fft_tile_bytes(reg_lanes, nb);
+  const uint64_t tiles = ((len + tile - 1) / tile) * std::max<size_t>(n_jobs, 1);
+  if (!L.global_work) {
+    L.smem = smem;
+    if (smem > 48 * 1024) RS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int per_sm = 0;
+    RS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFftThreads, smem));
+    L.grid = int(std::min<uint64_t>(tiles, uint64_t(std::max(per_sm, 1)) * sm_count()));
+  } else {
+    L.smem = 0;
+    L.grid = int(std::min<uint64_t>(tiles, uint64_t(2 * sm_count())));
+    const size_t need = size_t(L.grid) * rows * nb * 64;
+    if (st.scratch_bytes < need) {
+      if (st.scratch) {
+        RS_CUDA(cudaDeviceSynchronize());
+        cudaFree(st.scratch);
+        st.scratch = nullptr;
+        st.scratch_bytes = 0;
+      }
+      RS_CUDA(cudaMalloc(&st.scratch, need));
+      st.scratch_bytes = need;
+    }
+    L.args.scratch = st.scratch;
+  }
+  return RSGPU_OK;
 }
 
 template <class K>
@@ -872,6 +708,21 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
   a.mtrunc = st.mtrunc;
   a.last = st.last;
   a.mod = st.field->host.mod;
+  a.kbank = st.field->d_kbank;
+  fill_stages(a);
+  L.engine = leo_engine();
+  if (L.engine == 1) {
+    const bool b16f = st.field->bits == 16;
+    const size_t nj = jobs.size();
+    if (L.decode)
+      return b16f ? configure_fft(k_fft_decode<16, false>, L, st.n, st.n, len, nj)
+                  : configure_fft(k_fft_decode<8, false>, L, st.n, st.n, len, nj);
+    if (L.verify)
+      return b16f ? configure_fft(k_fft_encode<16, true, false>, L, 2 * st.m, st.m, len, nj)
+                  : configure_fft(k_fft_encode<8, true, false>, L, 2 * st.m, st.m, len, nj);
+    return b16f ? configure_fft(k_fft_encode<16, false, false>, L, 2 * st.m, st.m, len, nj)
+                : configure_fft(k_fft_encode<8, false, false>, L, 2 * st.m, st.m, len, nj);
+  }
   const uint32_t lanes = L.decode ? st.n : 2 * st.m;
   const uint32_t nb_guess = pick_nb(lanes, len);
   const uint64_t tiles = ((len + nb_guess * 64 - 1) / (nb_guess * 64)) * std::max<size_t>(jobs.size(), 1);
@@ -896,6 +747,32 @@ int leo_launch(const LeoLaunch &L, cudaStream_t s) {
   if (L.args.n_jobs == 0) return RSGPU_OK;
   const bool b16 = L.codec->leo->field->bits == 16;
   const LeoArgs &a = L.args;
+  if (L.engine == 1) {
+    const dim3 grid(L.grid), block(kFftThreads);
+#define FFT_GO(KERNEL) KERNEL<<<grid, block, L.smem, s>>>(a)
+    if (L.decode) {
+      if (L.global_work) {
+        if (b16) FFT_GO((k_fft_decode<16, true>)); else FFT_GO((k_fft_decode<8, true>));
+      } else {
+        if (b16) FFT_GO((k_fft_decode<16, false>)); else FFT_GO((k_fft_decode<8, false>));
+      }
+    } else if (L.verify) {
+      if (L.global_work) {
+        if (b16) FFT_GO((k_fft_encode<16, true, true>)); else FFT_GO((k_fft_encode<8, true, true>));
+      } else {
+        if (b16) FFT_GO((k_fft_encode<16, true, false>)); else FFT_GO((k_fft_encode<8, true, false>));
+      }
+    } else {
+      if (L.global_work) {
+        if (b16) FFT_GO((k_fft_encode<16, false, true>)); else FFT_GO((k_fft_encode<8, false, true>));
+      } else {
+        if (b16) FFT_GO((k_fft_encode<16, false, false>)); else FFT_GO((k_fft_encode<8, false, false>));
+      }
+    }
+#undef FFT_GO
+    launch_counter_add(1);
+    return cuda_status(cudaGetLastError());
+  }
   const dim3 grid(L.grid), block(kLeoThreads);
 #define LEO_GO(KERNEL) KERNEL<<<grid, block, L.smem, s>>>(a)
   if (L.decode) {
@@ -967,6 +844,162 @@ int leopard_verify(Codec &c, size_t n, const uint8_t *const *shards, size_t len,
 int leopard_reconstruct(Codec &c, size_t n, uint8_t *const *shards, const uint8_t *present, size_t len, int goal,
                         const uint8_t *required, size_t n_required, cudaStream_t s) {
   return run_once(c, RSGPU_OP_RECONSTRUCT, n, shards, present, len, goal, required, n_required, nullptr, s);
+}
+
+// ====================================================================== mixed batches
+int leopard_geometry(Codec &c, LeoGeometry *g) {
+  if (!c.leo) return RSGPU_ERR_INVALID_ARGUMENT;
+  const LeopardState &st = *c.leo;
+  g->bits = st.field->bits;
+  g->k = uint32_t(c.k);
+  g->p = uint32_t(c.m);
+  g->m = st.m;
+  g->n = st.n;
+  g->mtrunc = st.mtrunc;
+  g->last = st.last;
+  g->mod = st.field->host.mod;
+  g->skew = st.field->d_skew;
+  g->bank = st.field->d_bank;
+  g->kbank = st.field->d_kbank;
+  LeoArgs a{};
+  a.m = st.m;
+  a.n = st.n;
+  fill_stages(a);
+  g->st_ienc = a.st_ienc;
+  g->st_fenc = a.st_fenc;
+  g->st_idec = a.st_idec;
+  g->st_fdec = a.st_fdec;
+  g->n_ienc = a.n_ienc;
+  g->n_fenc = a.n_fenc;
+  g->n_idec = a.n_idec;
+  g->n_fdec = a.n_fdec;
+  return RSGPU_OK;
+}
+
+int leopard_locators(Codec &c, size_t n, const uint8_t *present, const uint16_t **err, uint32_t *input_count,
+                     cudaStream_t s) {
+  LeopardState &st = *c.leo;
+  const size_t total = c.k + c.m;
+  std::lock_guard<std::mutex> g(st.mu);
+  std::vector<std::pair<std::string, const uint8_t *>> pending;
+  std::vector<LeoPlan *> plans(n);
+  for (size_t i = 0; i < n; ++i) {
+    int rc = decode_plan(c, present + i * total, &plans[i], s, pending);
+    if (rc) return rc;
+  }
+  int rc = build_locators(c, pending, s);
+  if (rc) return rc;
+  // unordered_map nodes are stable, so the plan pointers are still valid.
+  for (size_t i = 0; i < n; ++i) {
+    err[i] = plans[i]->err;
+    input_count[i] = plans[i]->input_count;
+  }
+  return RSGPU_OK;
+}
+
+const uint8_t (*leopard_mul8())[256] {
+  static uint8_t mul[256][256];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    LeoField *f = nullptr;
+    if (leo_field(8, &f) != RSGPU_OK) return;
+    const LeoTables &t = f->host;
+    for (uint32_t a = 0; a < 256; ++a)
+      for (uint32_t b = 0; b < 256; ++b)
+        mul[a][b] = (a && b) ? uint8_t(t.exp[t.add_mod(t.log[a], t.log[b])]) : 0;
+  });
+  return mul;
+}
+
+namespace {
+
+// The element whose log is 0 (the multiplicative identity of the Leopard
+// field's representation).
+uint8_t leo8_one() {
+  LeoField *f = nullptr;
+  leo_field(8, &f);
+  return uint8_t(f->host.exp[0]);
+}
+
+}  // namespace
+
+int leopard_dense_encode(Codec &c, std::vector<uint8_t> &rows) {
+  LeopardState &st = *c.leo;
+  if (st.field->bits != 8) return RSGPU_ERR_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> g(st.mu);
+    if (!st.dense_enc.empty()) {
+      rows = st.dense_enc;
+      return RSGPU_OK;
+    }
+  }
+  // Encode the unit vectors: data shard j holds the identity element at
+  // column j, so parity shard r column j is coefficient (r, j) of the map.
+  const size_t k = c.k, m = c.m, total = k + m;
+  const size_t L = (k + 63) / 64 * 64;
+  std::vector<uint8_t> host(total * L, 0);
+  const uint8_t one = leo8_one();
+  for (size_t j = 0; j < k; ++j) host[j * L + j] = one;
+  uint8_t *d = nullptr;
+  RS_CUDA(cudaMalloc(&d, host.size()));
+  RS_CUDA(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
+  std::vector<uint8_t *> ptrs(total);
+  for (size_t i = 0; i < total; ++i) ptrs[i] = d + i * L;
+  int rc = leopard_encode(c, 1, ptrs.data(), L, nullptr);
+  if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpy(host.data(), d, host.size(), cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  if (rc) return rc;
+  rows.assign(m * k, 0);
+  for (size_t r = 0; r < m; ++r)
+    for (size_t j = 0; j < k; ++j) rows[r * k + j] = host[(k + r) * L + j];
+  std::lock_guard<std::mutex> g(st.mu);
+  st.dense_enc = rows;
+  return RSGPU_OK;
+}
+
+int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, std::vector<LeoDenseMap> &maps,
+                         cudaStream_t s) {
+  LeopardState &st = *c.leo;
+  if (st.field->bits != 8) return RSGPU_ERR_INVALID_ARGUMENT;
+  const size_t k = c.k, m = c.m, total = k + m;
+  maps.assign(n, LeoDenseMap{});
+  size_t max_in = 1;
+  for (size_t i = 0; i < n; ++i) {
+    const uint8_t *pr = present + i * total;
+    LeoDenseMap &mp = maps[i];
+    for (size_t x = 0; x < total; ++x) {
+      if (pr[x])
+        mp.inputs.push_back(uint16_t(x));
+      else if (goal == RSGPU_GOAL_ALL || x < k)
+        mp.targets.push_back(uint16_t(x));
+    }
+    max_in = std::max(max_in, mp.inputs.size());
+  }
+  // One reconstruction over unit-vector stripes: the q-th present shard of
+  // pattern i holds the identity element at column q, so target t column q
+  // is coefficient (t, q) of that pattern's map.
+  const size_t L = (max_in + 63) / 64 * 64;
+  std::vector<uint8_t> host(n * total * L, 0);
+  const uint8_t one = leo8_one();
+  for (size_t i = 0; i < n; ++i)
+    for (size_t q = 0; q < maps[i].inputs.size(); ++q) host[(i * total + maps[i].inputs[q]) * L + q] = one;
+  uint8_t *d = nullptr;
+  RS_CUDA(cudaMalloc(&d, host.size()));
+  RS_CUDA(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
+  std::vector<uint8_t *> ptrs(n * total);
+  for (size_t i = 0; i < n * total; ++i) ptrs[i] = d + i * L;
+  int rc = leopard_reconstruct(c, n, ptrs.data(), present, L, goal, nullptr, 0, s);
+  if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpy(host.data(), d, host.size(), cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  if (rc) return rc;
+  for (size_t i = 0; i < n; ++i) {
+    LeoDenseMap &mp = maps[i];
+    const size_t ni = mp.inputs.size();
+    mp.rows.assign(mp.targets.size() * ni, 0);
+    for (size_t t = 0; t < mp.targets.size(); ++t)
+      for (size_t q = 0; q < ni; ++q) mp.rows[t * ni + q] = host[(i * total + mp.targets[t]) * L + q];
+  }
+  return RSGPU_OK;
 }
 
 // ====================================================================== no allocation

@@ -7,6 +7,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <memory>
+#include <vector>
 
 namespace rsgpu {
 
@@ -36,6 +37,37 @@ int leopard_reconstruct(Codec &c, size_t n_stripes, uint8_t *const *shards, cons
 // No-allocation Leopard reconstruction (leopard.cu): static device buffers only.
 int leopard_reconstruct_noalloc(Codec &c, uint8_t *const *shards, const uint8_t *present, size_t len,
                                 cudaStream_t s);
+
+// ---- mixed batches (batch.cu)
+struct LeoGeometry {
+  int bits;
+  uint32_t k, p, m, n, mtrunc, last, mod;
+  const uint16_t *skew;
+  const uint32_t *bank;   // half-warp layer kernels
+  const uint32_t *kbank;  // register-stage kernels
+  uint32_t st_ienc, st_fenc, st_idec, st_fdec;  // stage plans (leo_types.hpp)
+  uint32_t n_ienc, n_fenc, n_idec, n_fdec;
+};
+int leopard_geometry(Codec &c, LeoGeometry *g);
+// Error locators of n presence patterns (k + m flags each), built on the GPU
+// for patterns not seen before; the pointers stay valid for the codec's life.
+int leopard_locators(Codec &c, size_t n, const uint8_t *present, const uint16_t **err, uint32_t *input_count,
+                     cudaStream_t s);
+// Leopard GF(2^8) products: mul[a][b] in the codec field's representation.
+const uint8_t (*leopard_mul8())[256];
+// The GF(2^8) Leopard encode as a dense m x k matrix over the Leopard field
+// (the FFT pipeline is linear, so applying this matrix gives the same bytes).
+int leopard_dense_encode(Codec &c, std::vector<uint8_t> &rows);
+// The GF(2^8) Leopard reconstruction of one presence pattern as a dense map
+// from the present shards (ascending) to the targets (ascending).  The
+// reference's decode uses every present shard, and so does this map, so the
+// bytes agree on any input, codeword or not.
+struct LeoDenseMap {
+  std::vector<uint16_t> inputs, targets;
+  std::vector<uint8_t> rows;  // targets x inputs
+};
+int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, std::vector<LeoDenseMap> &maps,
+                         cudaStream_t s);
 
 int tower_encode(Codec &c, size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s);
 int tower_verify(Codec &c, size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok,

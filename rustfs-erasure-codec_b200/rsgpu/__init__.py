@@ -61,6 +61,60 @@ class _Options(ctypes.Structure):
     ]
 
 
+class MixOp(ctypes.Structure):
+    """rsgpu_mix_op: one operation of a mixed batch."""
+    _fields_ = [
+        ("codec", ctypes.c_void_p),
+        ("op", ctypes.c_int32),
+        ("goal", ctypes.c_int32),
+        ("shards", ctypes.c_void_p),
+        ("present", ctypes.c_void_p),
+        ("shard_len", ctypes.c_size_t),
+    ]
+
+
+class Plan(ctypes.Structure):
+    """rsgpu_plan: algorithm (ALGO_APPLY / ALGO_FFT) and tile."""
+    _fields_ = [("algo", ctypes.c_int32), ("tile", ctypes.c_int32)]
+
+    def tuple(self):
+        return (int(self.algo), int(self.tile))
+
+
+class MixOptions(ctypes.Structure):
+    _fields_ = [("planner", ctypes.c_int32), ("order", ctypes.c_int32), ("graph", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32)]
+
+
+class MixInfo(ctypes.Structure):
+    _fields_ = [("n_ops", ctypes.c_size_t), ("n_jobs", ctypes.c_size_t), ("n_items", ctypes.c_size_t),
+                ("n_classes", ctypes.c_size_t), ("algorithmic_bytes", ctypes.c_uint64),
+                ("device_bytes", ctypes.c_size_t), ("grid", ctypes.c_uint32), ("smem_bytes", ctypes.c_uint32),
+                ("kernels_per_launch", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+
+
+class TuneOptions(ctypes.Structure):
+    _fields_ = [("target_bytes", ctypes.c_size_t), ("repeats", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+MODEL_FEATURES, MODEL_PLANS, MODEL_HIDDEN = 11, 6, 32
+
+
+class TuneSample(ctypes.Structure):
+    _fields_ = [("features", ctypes.c_float * MODEL_FEATURES), ("plan", Plan), ("gbps", ctypes.c_float)]
+
+
+class TrainOptions(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("lr", ctypes.c_float), ("seed", ctypes.c_uint64)]
+
+
+ALGO_APPLY, ALGO_FFT = 0, 1
+# Order of the cost model's outputs (rsgpu_plan_index).
+MODEL_PLAN_ORDER = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (1, 3)]
+PLANNER = {"fixed": 0, "table": 1, "model": 2}
+ORDER = {"submit": 0, "cost": 1}
+
+
 class CacheStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in
                 ("requests", "hits", "misses", "inserts", "evictions", "entries", "retained_bytes")]
@@ -115,6 +169,31 @@ def _lib():
             "rsgpu_batch_kernel_count": (ctypes.c_uint32, [P]),
             "rsgpu_batch_free": (None, [P]),
             "rsgpu_leopard_reconstruct_noalloc": (I32, [P, PP, SZP, U8P, SZ, P]),
+            "rsgpu_mix_options_default": (None, [ctypes.POINTER(MixOptions)]),
+            "rsgpu_mix_prepare": (I32, [P, SZ, ctypes.POINTER(MixOptions), PP]),
+            "rsgpu_mix_prepare_planned": (I32, [P, SZ, P, ctypes.POINTER(MixOptions), PP]),
+            "rsgpu_mix_launch": (I32, [P, P]),
+            "rsgpu_mix_results": (I32, [P, U8P, P]),
+            "rsgpu_mix_get_info": (I32, [P, ctypes.POINTER(MixInfo)]),
+            "rsgpu_mix_get_plans": (I32, [P, P, SZ]),
+            "rsgpu_mix_free": (None, [P]),
+            "rsgpu_plan_features": (I32, [P, P]),
+            "rsgpu_plan_index": (I32, [Plan]),
+            "rsgpu_tune": (I32, [P, SZ, ctypes.POINTER(TuneOptions), SZP]),
+            "rsgpu_tuner_samples": (SZ, [P, SZ]),
+            "rsgpu_tuner_table_size": (SZ, []),
+            "rsgpu_tuner_lookup": (I32, [P, ctypes.POINTER(Plan)]),
+            "rsgpu_tuner_save": (I32, [ctypes.c_char_p]),
+            "rsgpu_tuner_load": (I32, [ctypes.c_char_p]),
+            "rsgpu_tuner_clear": (None, []),
+            "rsgpu_model_param_count": (SZ, []),
+            "rsgpu_model_get_params": (I32, [P, SZ]),
+            "rsgpu_model_set_params": (I32, [P, SZ]),
+            "rsgpu_model_train": (I32, [P, P, P, SZ, ctypes.POINTER(TrainOptions), ctypes.POINTER(ctypes.c_float)]),
+            "rsgpu_model_train_from_tuner": (I32, [ctypes.POINTER(TrainOptions), ctypes.POINTER(ctypes.c_float)]),
+            "rsgpu_model_predict": (I32, [P, SZ, P]),
+            "rsgpu_model_gradients": (I32, [P, P, P, P, SZ, ctypes.POINTER(ctypes.c_float), P]),
+            "rsgpu_model_ready": (I32, []),
             "rsgpu_kernel_launch_count": (ctypes.c_uint64, []),
             "rsgpu_error_string": (ctypes.c_char_p, [I32]),
             "rsgpu_version": (ctypes.c_char_p, []),
@@ -289,9 +368,207 @@ class PreparedBatch:
         return int(_lib().rsgpu_batch_kernel_count(self._h))
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            _lib().rsgpu_batch_free(self._h)
+        h = getattr(self, "_h", None)
+        if h and _L is not None and getattr(_L, "rsgpu_batch_free", None) is not None:
+            _L.rsgpu_batch_free(h)
             self._h = None
+
+
+def _mix_ops(ops, keep):
+    """ctypes array of rsgpu_mix_op for a list of op dicts (see MixedBatch)."""
+    n = len(ops)
+    arr = (MixOp * max(n, 1))()
+    for i, o in enumerate(ops):
+        codec = o["codec"]
+        ptrs = np.array([s.data_ptr() if hasattr(s, "data_ptr") else int(s) for s in o["shards"]], np.uint64)
+        keep += [codec, ptrs, o["shards"]]
+        arr[i].codec = codec._h
+        arr[i].op = OP[o["op"]]
+        arr[i].goal = GOAL[o.get("goal", "all")]
+        arr[i].shards = ptrs.ctypes.data
+        if o["op"] == "reconstruct":
+            pres = np.ascontiguousarray(np.asarray(o["present"], dtype=np.uint8))
+            keep.append(pres)
+            arr[i].present = pres.ctypes.data
+        arr[i].shard_len = int(o["shard_len"])
+    return arr
+
+
+class MixedBatch:
+    """A mixed batch (rsgpu_mix_prepare in include/rsgpu.h): operations of
+    different codecs, shard lengths and kinds in one persistent kernel.
+
+    ``ops`` is a list of dicts with keys ``codec`` (ReedSolomon), ``op``
+    ("encode" / "reconstruct" / "verify"), ``shards`` (k + m device pointers,
+    or torch CUDA tensors), ``shard_len``, and for reconstruct ``present`` (k + m
+    flags) and ``goal`` ("all" / "data").  ``plans`` optionally forces a plan
+    (algo, tile) per operation."""
+
+    def __init__(self, ops, planner: str = "fixed", order: str = "cost", graph: bool = True, ctas_per_sm: int = 0,
+                 plans=None):
+        self._keep = []
+        n = len(ops)
+        arr = _mix_ops(ops, self._keep)
+        self._arr = arr
+        self.n_ops = n
+        opts = MixOptions()
+        _lib().rsgpu_mix_options_default(ctypes.byref(opts))
+        opts.planner = PLANNER[planner]
+        opts.order = ORDER[order]
+        opts.graph = 1 if graph else 0
+        opts.ctas_per_sm = int(ctas_per_sm)
+        h = ctypes.c_void_p()
+        if plans is None:
+            rc = _lib().rsgpu_mix_prepare(ctypes.addressof(arr), n, ctypes.byref(opts), ctypes.byref(h))
+        else:
+            parr = (Plan * max(n, 1))(*[Plan(int(a), int(t)) for a, t in plans])
+            rc = _lib().rsgpu_mix_prepare_planned(ctypes.addressof(arr), n, ctypes.addressof(parr),
+                                                  ctypes.byref(opts), ctypes.byref(h))
+        _check(rc)
+        self._h = h
+
+    @staticmethod
+    def _stream():
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+
+    def launch(self, stream=None) -> None:
+        _check(_lib().rsgpu_mix_launch(self._h, self._stream() if stream is None else stream))
+
+    def results(self) -> np.ndarray:
+        ok = np.zeros(max(1, self.n_ops), np.uint8)
+        _check(_lib().rsgpu_mix_results(self._h, ok.ctypes.data_as(U8P), self._stream()))
+        return ok[: self.n_ops].astype(bool)
+
+    def info(self) -> MixInfo:
+        out = MixInfo()
+        _check(_lib().rsgpu_mix_get_info(self._h, ctypes.byref(out)))
+        return out
+
+    def plans(self) -> List[tuple]:
+        parr = (Plan * max(self.n_ops, 1))()
+        _check(_lib().rsgpu_mix_get_plans(self._h, ctypes.addressof(parr), self.n_ops))
+        return [parr[i].tuple() for i in range(self.n_ops)]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _L is not None and getattr(_L, "rsgpu_mix_free", None) is not None:
+            _L.rsgpu_mix_free(h)
+            self._h = None
+
+
+class Tuner:
+    """The process-wide plan table and cost model (rsgpu_tune, rsgpu_model_*
+    in include/rsgpu.h).  Every call runs on the GPU through librsgpu.so."""
+
+    @staticmethod
+    def features(op: dict) -> np.ndarray:
+        keep = []
+        arr = _mix_ops([op], keep)
+        out = np.zeros(MODEL_FEATURES, np.float32)
+        _check(_lib().rsgpu_plan_features(ctypes.addressof(arr), out.ctypes.data))
+        return out
+
+    @staticmethod
+    def tune(ops, target_bytes: int = 0, repeats: int = 0) -> int:
+        keep = []
+        arr = _mix_ops(ops, keep)
+        o = TuneOptions(int(target_bytes), int(repeats), 0)
+        done = ctypes.c_size_t()
+        _check(_lib().rsgpu_tune(ctypes.addressof(arr), len(ops), ctypes.byref(o), ctypes.byref(done)))
+        return int(done.value)
+
+    @staticmethod
+    def lookup(op: dict):
+        keep = []
+        arr = _mix_ops([op], keep)
+        p = Plan()
+        rc = _lib().rsgpu_tuner_lookup(ctypes.addressof(arr), ctypes.byref(p))
+        if rc == 13:
+            return None
+        _check(rc)
+        return p.tuple()
+
+    @staticmethod
+    def samples():
+        n = int(_lib().rsgpu_tuner_samples(None, 0))
+        arr = (TuneSample * max(n, 1))()
+        n = int(_lib().rsgpu_tuner_samples(ctypes.addressof(arr), n))
+        return [(np.array(arr[i].features[:], np.float32), arr[i].plan.tuple(), float(arr[i].gbps)) for i in range(n)]
+
+    @staticmethod
+    def table_size() -> int:
+        return int(_lib().rsgpu_tuner_table_size())
+
+    @staticmethod
+    def save(path: str) -> None:
+        _check(_lib().rsgpu_tuner_save(path.encode()))
+
+    @staticmethod
+    def load(path: str) -> None:
+        _check(_lib().rsgpu_tuner_load(path.encode()))
+
+    @staticmethod
+    def clear() -> None:
+        _lib().rsgpu_tuner_clear()
+
+    # ---- cost model
+    @staticmethod
+    def param_count() -> int:
+        return int(_lib().rsgpu_model_param_count())
+
+    @staticmethod
+    def model_ready() -> bool:
+        return bool(_lib().rsgpu_model_ready())
+
+    @staticmethod
+    def get_params() -> np.ndarray:
+        out = np.zeros(Tuner.param_count(), np.float32)
+        _check(_lib().rsgpu_model_get_params(out.ctypes.data, out.size))
+        return out
+
+    @staticmethod
+    def set_params(w) -> None:
+        w = np.ascontiguousarray(w, np.float32)
+        _check(_lib().rsgpu_model_set_params(w.ctypes.data, w.size))
+
+    @staticmethod
+    def train(x, y, mask, epochs=0, lr=0.0, seed=1) -> float:
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        mask = np.ascontiguousarray(mask, np.uint8)
+        loss = ctypes.c_float()
+        o = TrainOptions(int(epochs), float(lr), int(seed))
+        _check(_lib().rsgpu_model_train(x.ctypes.data, y.ctypes.data, mask.ctypes.data, x.shape[0], ctypes.byref(o),
+                                        ctypes.byref(loss)))
+        return float(loss.value)
+
+    @staticmethod
+    def train_from_tuner(epochs=0, lr=0.0, seed=1) -> float:
+        loss = ctypes.c_float()
+        o = TrainOptions(int(epochs), float(lr), int(seed))
+        _check(_lib().rsgpu_model_train_from_tuner(ctypes.byref(o), ctypes.byref(loss)))
+        return float(loss.value)
+
+    @staticmethod
+    def predict(x) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.zeros((x.shape[0], MODEL_PLANS), np.float32)
+        _check(_lib().rsgpu_model_predict(x.ctypes.data, x.shape[0], out.ctypes.data))
+        return out
+
+    @staticmethod
+    def gradients(params, x, y, mask):
+        params = np.ascontiguousarray(params, np.float32)
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        mask = np.ascontiguousarray(mask, np.uint8)
+        loss = ctypes.c_float()
+        g = np.zeros_like(params)
+        _check(_lib().rsgpu_model_gradients(params.ctypes.data, x.ctypes.data, y.ctypes.data, mask.ctypes.data,
+                                            x.shape[0], ctypes.byref(loss), g.ctypes.data))
+        return float(loss.value), g
 
 
 class ReedSolomon:
