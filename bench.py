@@ -32,6 +32,7 @@ SEED = 0x00EC5EED20260524  # the reference benches' BASE_SEED (benches/common/mo
 GEOMS = [(10, 4), (16, 4)]
 SHARD = 1 << 20
 STRIPES = 4096
+MIX_OPS = 16384  # stripes of the mixed-geometry workload
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 PROFILE_FILE = os.path.join(ROOT, "profiles", "k_apply_vec_encode_10x4.txt")
 
@@ -266,6 +267,9 @@ def main():
     ap.add_argument("--stripes", type=int, default=STRIPES)
     ap.add_argument("--e2e-stripes", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mix", action="store_true", help="skip the mixed-geometry workload")
+    ap.add_argument("--mix-ops", type=int, default=MIX_OPS)
+    ap.add_argument("--retune", action="store_true", help="re-run the autotuner instead of loading its table")
     ap.add_argument("--case", default=None, choices=sorted(PROFILE_CASES),
                     help="run one small profiling case (three launches of one kernel) and exit")
     args = ap.parse_args()
@@ -428,6 +432,16 @@ def main():
     # End to end through the public API with pinned host buffers.
     e2e = e2e_measure(torch, rsgpu, args, rank)
 
+    # Mixed geometries in one persistent kernel (batched, model-scheduled)
+    # against the per-stripe kernel loop.
+    mixed = None
+    if not args.no_mix:
+        for item in work:
+            item.clear()  # drops the config-2 shard buffers (137 GiB)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        mixed = mixed_workload(args, torch, rsgpu, rank, stream, gen)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -454,6 +468,7 @@ def main():
                            "batched_same_stripes": round(batched_same, 1),
                            "batched_speedup": round(batched_same / ps_value, 3)},
             "clocks": clk.summary(),
+            "mixed": mixed,
             "e2e": e2e,
             "gpu_launches": gpu_launches,
             "cpu_baseline": cpu,
@@ -463,6 +478,143 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def mixed_workload(args, torch, rsgpu, rank, stream, gen):
+    """16384 stripes: geometries uniform over classic GF(2^8) {4+2, 6+3, 8+4,
+    12+4, 16+4} and Leopard GF(2^8) {32+16, 128+64}; shard sizes log-uniform
+    4 KiB..4 MiB (64-byte multiples); erasures uniform 0..m; encode /
+    reconstruct / verify with probabilities 0.5 / 0.4 / 0.1 (rsgpu.workload).
+    The stripes do not fit HBM at once (~0.4 TB), so they run in waves that
+    share one arena (a wave's inputs are whatever the previous wave left
+    there); every mode runs the same waves in the same order.
+
+    Modes, all on device-resident shards, timed with CUDA events:
+      batched_model: one persistent-kernel mixed batch per wave (CUDA graph),
+                     plans from the measured table + cost model;
+      batched_fixed: the same with the fixed plan rule;
+      per_stripe:    one prepared launch per stripe and operation (the codec's
+                     own kernels, the plain per-stripe loop);
+      per_stripe_api: one rsgpu_encode / _reconstruct / _verify call per stripe.
+    """
+    import ctypes
+
+    from rsgpu import tune_mix
+    from rsgpu import workload as W
+
+    specs = W.mixed_specs(args.mix_ops, SEED + 4 + 1000 * rank)
+    free, _ = torch.cuda.mem_get_info()
+    arena_bytes = int(min(free * 0.5, 80e9))
+    groups = W.waves(specs, arena_bytes)
+    size = max(W.layout(specs, g)[1] for g in groups)
+    arena = torch.empty(size + 4096, dtype=torch.uint8, device="cuda")
+    arena.random_(0, 256, generator=gen)
+    base = arena.data_ptr()
+    codecs = tune_mix.make_codecs(W.MIX_GEOMETRIES)
+    T = rsgpu.Tuner
+    T.clear()
+    t0 = time.perf_counter()
+    if os.path.exists(tune_mix.DEFAULT_TABLE) and not args.retune:
+        T.load(tune_mix.DEFAULT_TABLE)
+        table_src = "loaded " + os.path.relpath(tune_mix.DEFAULT_TABLE, ROOT)
+    else:
+        sample = tune_mix.class_sample(W.mixed_specs(20000, 0x5EED), codecs, 160)
+        T.tune(sample, target_bytes=96 << 20, repeats=2)
+        table_src = "tuned in-process"
+    tune_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss = T.train_from_tuner(epochs=3000, lr=3e-3, seed=1)
+    train_s = time.perf_counter() - t0
+
+    waves, abytes = [], 0
+    t0 = time.perf_counter()
+    for g in groups:
+        off, _ = W.layout(specs, g)
+        ops = []
+        for i in g:
+            s = specs[i]
+            ops.append(tune_mix.spec_op(s, codecs, [base + off[i] + j * s.shard_len for j in range(s.total)]))
+        bm = rsgpu.MixedBatch(ops, planner="model", graph=True)
+        bf = rsgpu.MixedBatch(ops, planner="fixed", graph=True)
+        abytes += bm.info().algorithmic_bytes
+        per = []
+        for o in ops:
+            if o["op"] == "reconstruct" and np.asarray(o["present"]).all():
+                continue
+            ptrs = np.array(o["shards"], np.uint64)
+            pres = None if o["op"] != "reconstruct" else np.asarray(o["present"], np.uint8)[None, :]
+            per.append(o["codec"].prepare_batch(o["op"], ptrs, o["shard_len"], present=pres))
+        waves.append(dict(ops=ops, model=bm, fixed=bf, per=per))
+    prep_s = time.perf_counter() - t0
+    plans = {}
+    for w in waves:
+        for p in w["model"].plans():
+            plans[p] = plans.get(p, 0) + 1
+
+    def run(mode):
+        lat = []
+        for w in waves:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if mode == "per":
+                for pb in w["per"]:
+                    pb.launch()
+            else:
+                w[mode].launch()
+            e1.record(stream)
+            lat.append((e0, e1))
+        return lat
+
+    out = {"workload": f"{args.mix_ops} stripes, 7 geometries (classic GF8 4+2/6+3/8+4/12+4/16+4, Leopard GF8 "
+                       "32+16/128+64), shards 4 KiB-4 MiB log-uniform, erasures 0..m, enc/rec/ver 0.5/0.4/0.1",
+           "waves": len(waves), "algorithmic_bytes": int(abytes), "unit": "GB/s",
+           "planner": {"table": table_src, "classes": T.table_size(), "samples": len(T.samples()),
+                       "model_loss": round(loss, 4), "tune_s": round(tune_s, 1), "train_s": round(train_s, 2),
+                       "prepare_s": round(prep_s, 1),
+                       "plans": {f"{'apply' if a == 0 else 'fft'}{t}": c for (a, t), c in sorted(plans.items())}}}
+    steps = max(1, min(args.steps, 5))
+    for mode, key in [("model", "batched_model"), ("fixed", "batched_fixed"), ("per", "per_stripe")]:
+        run(mode)
+        torch.cuda.synchronize()
+        times, wave_ms = [], []
+        for _ in range(steps):
+            lat = run(mode)
+            torch.cuda.synchronize()
+            times.append(lat[0][0].elapsed_time(lat[-1][1]))
+            wave_ms += [a.elapsed_time(b) for a, b in lat]
+        ms = float(np.median(times))
+        out[key] = {"value": round(abytes / (ms / 1e3) / 1e9, 1), "ms_per_pass": round(ms, 2),
+                    "wave_ms_p50": round(float(np.percentile(wave_ms, 50)), 2),
+                    "wave_ms_p99": round(float(np.percentile(wave_ms, 99)), 2)}
+    # One pass of the per-stripe public API (host-side call per stripe).
+    L = rsgpu.lib()
+    st = stream.cuda_stream
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for w in waves:
+        for o in w["ops"]:
+            n = len(o["shards"])
+            ptrs = (ctypes.c_void_p * n)(*o["shards"])
+            lens = (ctypes.c_size_t * n)(*([o["shard_len"]] * n))
+            c = o["codec"]._h
+            if o["op"] == "encode":
+                rc = L.rsgpu_encode(c, ptrs, lens, n, 1, st)
+            elif o["op"] == "verify":
+                ok = ctypes.c_int32()
+                rc = L.rsgpu_verify(c, ptrs, lens, n, ctypes.byref(ok), 1, st)
+            else:
+                pres = (ctypes.c_uint8 * n)(*np.asarray(o["present"]).tolist())
+                rc = L.rsgpu_reconstruct(c, ptrs, lens, pres, n, 0, None, 0, 1, st)
+            assert rc == 0, rc
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    out["per_stripe_api"] = {"value": round(abytes / dt / 1e9, 1), "s_per_pass": round(dt, 2)}
+    out["speedup_vs_per_stripe"] = round(out["batched_model"]["value"] / out["per_stripe"]["value"], 3)
+    out["speedup_vs_per_stripe_api"] = round(out["batched_model"]["value"] / out["per_stripe_api"]["value"], 3)
+    del waves, arena
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
 
 
 def e2e_measure(torch, rsgpu, args, rank):
