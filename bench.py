@@ -270,6 +270,10 @@ def main():
     ap.add_argument("--no-mix", action="store_true", help="skip the mixed-geometry workload")
     ap.add_argument("--mix-ops", type=int, default=MIX_OPS)
     ap.add_argument("--retune", action="store_true", help="re-run the autotuner instead of loading its table")
+    ap.add_argument("--no-serve", action="store_true", help="skip the request-server workload")
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-loads", type=float, nargs="+", default=[50.0, 200.0, 800.0],
+                    help="offered loads (GB/s of algorithmic bytes) of the Poisson request stream")
     ap.add_argument("--case", default=None, choices=sorted(PROFILE_CASES),
                     help="run one small profiling case (three launches of one kernel) and exit")
     args = ap.parse_args()
@@ -441,6 +445,13 @@ def main():
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
         mixed = mixed_workload(args, torch, rsgpu, rank, stream, gen)
+    serving = None
+    if not args.no_serve:
+        for item in work:
+            item.clear()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        serving = serving_workload(args, torch, rsgpu, rank, gen)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -469,6 +480,7 @@ def main():
                            "batched_speedup": round(batched_same / ps_value, 3)},
             "clocks": clk.summary(),
             "mixed": mixed,
+            "serving": serving,
             "e2e": e2e,
             "gpu_launches": gpu_launches,
             "cpu_baseline": cpu,
@@ -612,6 +624,78 @@ def mixed_workload(args, torch, rsgpu, rank, stream, gen):
     out["speedup_vs_per_stripe"] = round(out["batched_model"]["value"] / out["per_stripe"]["value"], 3)
     out["speedup_vs_per_stripe_api"] = round(out["batched_model"]["value"] / out["per_stripe_api"]["value"], 3)
     del waves, arena
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
+def serving_workload(args, torch, rsgpu, rank, gen):
+    """Requests of the mixed workload plus Leopard GF(2^16) 2048+1024 at
+    8 KiB shards (one request in eight), arriving as a seeded Poisson stream
+    at a sweep of offered loads, served by the request server (continuous
+    batching, model planner with the measured table, admission by a device
+    memory budget) on device-resident shards.  Reports per-request latency
+    p50 / p99 (submit -> completion) and GB/s of algorithmic bytes; the arena
+    checksum after every load level must be identical (no byte differs
+    whatever the batching)."""
+    from rsgpu import tune_mix
+    from rsgpu import workload as W
+
+    rng = np.random.default_rng(SEED + 5 + 1000 * rank)
+    specs = W.mixed_specs(args.serve_requests, SEED + 6 + 1000 * rank)
+    wide = ("leopard_gf16", 2048, 1024)
+    for i, s in enumerate(specs):
+        if rng.integers(8) == 0:
+            op = W.OPS[int(rng.choice(3, p=np.asarray(W.OP_PROBS, float)))]
+            present = None
+            if op == "reconstruct":
+                e = int(rng.integers(0, 1025))
+                present = np.ones(3072, np.uint8)
+                present[rng.choice(3072, size=e, replace=False)] = 0
+            specs[i] = W.MixOpSpec(wide, op, 8192, present)
+    codecs = tune_mix.make_codecs(W.MIX_GEOMETRIES + [wide])
+    idx = list(range(len(specs)))
+    off, size = W.layout(specs, idx)
+    arena = torch.empty(size + 4096, dtype=torch.uint8, device="cuda")
+    arena.random_(0, 256, generator=gen)
+    base = arena.data_ptr()
+    ptrs = [[base + off[i] + j * s.shard_len for j in range(s.total)] for i, s in enumerate(specs)]
+    abytes = np.array([s.algorithmic_bytes() for s in specs], np.float64)
+    mean_bytes = float(abytes.mean())
+    out = {"workload": f"{len(specs)} requests: mixed workload + Leopard GF16 2048+1024 at 8 KiB (1 in 8), "
+                       "Poisson arrivals, device-resident shards",
+           "unit": "GB/s", "levels": []}
+    budget = 16 << 30
+    sums = []
+    for load in args.serve_loads:
+        lam = load * 1e9 / mean_bytes
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(specs)))
+        srv = rsgpu.Server(device_budget=budget, streams=3, max_batch=512, planner="model")
+        comps = []
+        t0 = time.perf_counter()
+        for i, s in enumerate(specs):
+            while time.perf_counter() - t0 < arrivals[i]:
+                pass
+            srv.submit(codecs[s.geom], s.op, ptrs[i], s.shard_len, present=s.present, tag=i + 1)
+            if i % 64 == 0:
+                comps += srv.poll(timeout_ms=0)
+        comps += srv.wait(len(specs) - len(comps))
+        st = srv.stats()
+        srv.close()
+        assert all(c["status"] == 0 for c in comps)
+        lat = np.array([c["done_s"] - c["submit_s"] for c in comps]) * 1e3
+        span = max(c["done_s"] for c in comps) - min(c["submit_s"] for c in comps)
+        torch.cuda.synchronize()
+        sums.append(int(arena.view(torch.int64).sum().item()))
+        out["levels"].append({"offered_gbs": load, "achieved_gbs": round(float(abytes.sum()) / span / 1e9, 1),
+                              "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                              "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                              "launches": int(st["launches"]),
+                              "max_concurrent_launches": int(st["max_concurrent_launches"]),
+                              "max_reserved_gib": round(st["max_reserved_bytes"] / 2**30, 2)})
+    out["budget_gib"] = budget / 2**30
+    out["identical_across_loads"] = len(set(sums)) == 1
+    del arena
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     return out

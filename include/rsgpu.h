@@ -360,6 +360,62 @@ int32_t rsgpu_model_gradients(const float *params, const float *features, const 
                               size_t n, float *loss, float *grads);
 int32_t rsgpu_model_ready(void);
 
+/* ------------------------------------------------------------ request server */
+/* Continuous batching of encode / reconstruct / verify requests onto the GPU.
+ * Submit from any thread; a worker thread admits pending requests in arrival
+ * order while a request slot and the device-memory budget allow (a request
+ * holds (k + m) * shard_len bytes while admitted), runs everything admitted
+ * since the last launch as ONE mixed batch (plans from `planner`) on the next
+ * free of `streams` launch streams, and reports completions.  Launches overlap
+ * on the device; requests arriving meanwhile join the next launch.
+ * Host-memory requests (pinned memory recommended) are staged through device
+ * memory: inputs in, outputs (parity, rebuilt shards) back into the caller's
+ * buffers; device-memory requests (shards resident in HBM) run in place.
+ * Shard buffers must stay untouched until the request completes.  Results
+ * are byte-identical to the per-call entry points whatever else is in the
+ * batch.  No reference counterpart: the reference is called once per stripe
+ * by the storage node's own request handlers. */
+typedef struct rsgpu_server rsgpu_server;
+typedef struct rsgpu_server_options {
+  size_t device_budget;  /* bytes admitted requests may hold (0: half of free memory) */
+  uint32_t max_inflight; /* requests admitted at once (0: 4096) */
+  uint32_t max_batch;    /* requests per launch (0: 1024) */
+  uint32_t streams;      /* launches in flight at once (0: 3) */
+  int32_t planner;       /* RSGPU_PLANNER_* (default MODEL) */
+} rsgpu_server_options;
+typedef struct rsgpu_request {
+  const rsgpu_codec *codec;
+  int32_t op;              /* RSGPU_OP_* */
+  int32_t goal;            /* reconstruct: RSGPU_GOAL_ALL or _DATA */
+  uint8_t *const *shards;  /* k + m pointers (copied at submit) */
+  const uint8_t *present;  /* reconstruct: k + m flags (copied at submit) */
+  size_t shard_len;
+  int32_t mem;             /* RSGPU_MEM_HOST or RSGPU_MEM_DEVICE */
+  int32_t pad;
+  uint64_t tag;            /* returned with the completion */
+} rsgpu_request;
+typedef struct rsgpu_completion {
+  uint64_t tag;
+  int32_t status;  /* 0 or an error code */
+  int32_t ok;      /* verify: 1 when the parity matched, 0 otherwise; others 1 */
+  double submit_s, admit_s, done_s; /* seconds since the server started */
+} rsgpu_completion;
+typedef struct rsgpu_server_stats {
+  uint64_t submitted, completed, launches;
+  size_t pending, inflight, budget_bytes, reserved_bytes, max_reserved_bytes;
+  uint32_t max_concurrent_launches, pad;
+} rsgpu_server_stats;
+void rsgpu_server_options_default(rsgpu_server_options *out);
+int32_t rsgpu_server_new(const rsgpu_server_options *opts, rsgpu_server **out);
+/* Validation errors (reference precedence) return immediately; a request
+ * larger than the whole budget gets RSGPU_ERR_OUT_OF_MEMORY. */
+int32_t rsgpu_server_submit(rsgpu_server *s, const rsgpu_request *r);
+/* Up to `cap` completions; waits up to timeout_ms (-1: until one arrives). */
+size_t rsgpu_server_poll(rsgpu_server *s, rsgpu_completion *out, size_t cap, int32_t timeout_ms);
+int32_t rsgpu_server_get_stats(rsgpu_server *s, rsgpu_server_stats *out);
+/* Finishes every submitted request, then stops. */
+void rsgpu_server_free(rsgpu_server *s);
+
 /* ------------------------------------------------------------ no-allocation path */
 /* Leopard reconstruction (every missing shard, like rsgpu_reconstruct with
  * RSGPU_GOAL_ALL and RSGPU_MEM_DEVICE) that allocates no memory at all.  It

@@ -249,15 +249,31 @@ struct MixBatch {
   cudaGraphExec_t exec = nullptr;
   rsgpu_mix_info info{};
   std::vector<uint32_t *> owned_tables;  // private copies of classic decode tables
+  // Stream-ordered batches (one-shot launches of the request server): device
+  // memory comes from cudaMallocAsync on `stream` and goes back with
+  // cudaFreeAsync after the work queued there, so neither building nor
+  // freeing the batch synchronizes the device.
+  cudaStream_t stream = nullptr;
+  bool stream_ordered = false;
   ~MixBatch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    if (stream_ordered) {
+      for (void *p : {(void *)d_blob, (void *)d_flags, (void *)d_counter, (void *)d_scratch})
+        if (p) cudaFreeAsync(p, stream);
+      return;
+    }
     if (d_blob || d_flags || d_counter || d_scratch) cudaDeviceSynchronize();
     if (d_blob) cudaFree(d_blob);
     if (d_flags) cudaFree(d_flags);
     if (d_counter) cudaFree(d_counter);
     if (d_scratch) cudaFree(d_scratch);
     for (uint32_t *t : owned_tables) cudaFree(t);
+  }
+  template <class T>
+  cudaError_t alloc(T **p, size_t bytes) {
+    return stream_ordered ? cudaMallocAsync(reinterpret_cast<void **>(p), bytes, stream)
+                          : cudaMalloc(reinterpret_cast<void **>(p), bytes);
   }
 
   int enqueue(cudaStream_t s) const {
@@ -356,7 +372,7 @@ int add_apply_job(MixBuild &B, const rsgpu_plan &plan, bool verify, size_t n_in,
 }  // namespace
 
 int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, const rsgpu_mix_options &opt,
-              MixPtr &out) {
+              MixPtr &out, cudaStream_t ordered) {
   int device = 0;
   RS_CUDA(cudaGetDevice(&device));
   for (size_t i = 0; i < n_ops; ++i) {
@@ -365,6 +381,11 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   }
   MixPtr batch(new MixBatch());
   MixBatch &b = *batch;
+  if (ordered) {
+    if (opt.graph) return RSGPU_ERR_INVALID_ARGUMENT;
+    b.stream = ordered;
+    b.stream_ordered = true;
+  }
   b.n_ops = n_ops;
   b.plans.resize(n_ops);
   for (size_t i = 0; i < n_ops; ++i) {
@@ -381,7 +402,9 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   }
 
   MixBuild B;
-  cudaStream_t s = nullptr;
+  // Decode tables and locators are built on the batch's stream when it has
+  // one, so they precede its launch in stream order.
+  cudaStream_t s = b.stream_ordered ? b.stream : nullptr;
   // ---- classic reconstructions: plans and decode tables per codec, in one
   // K3 launch per codec.
   std::map<const Codec *, std::vector<size_t>> classic_rec;
@@ -408,9 +431,17 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
       pp.push_back(&cplans[i]);
     }
     std::vector<const uint32_t *> tbls;
-    uint32_t *owned = nullptr;
-    int rc = c.decode_tables_copy(pp, tbls, &owned, s);
-    if (owned) b.owned_tables.push_back(owned);
+    int rc;
+    if (b.stream_ordered) {
+      // A one-shot batch may use the cache's blocks in place: an evicted
+      // block is recycled only after a device-wide synchronization, which
+      // cannot happen before this launch has finished.
+      rc = c.decode_tables_shared(pp, tbls, s);
+    } else {
+      uint32_t *owned = nullptr;
+      rc = c.decode_tables_copy(pp, tbls, &owned, s);
+      if (owned) b.owned_tables.push_back(owned);
+    }
     if (rc) return rc;
     for (size_t x = 0; x < kv.second.size(); ++x) ctbl[kv.second[x]] = tbls[x];
   }
@@ -648,10 +679,13 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   const size_t o_roles = align256(o_leo + B.leo_jobs.size() * sizeof(LeoJob));
   const size_t o_tbl = align256(o_roles + B.roles.size());
   const size_t total_bytes = o_tbl + B.tables.size() * 4 + 256;
-  RS_CUDA(cudaMalloc(&b.d_blob, total_bytes));
-  RS_CUDA(cudaMalloc(&b.d_flags, std::max<size_t>(n_ops, 1) * 4));
-  RS_CUDA(cudaMemset(b.d_flags, 0, std::max<size_t>(n_ops, 1) * 4));
-  RS_CUDA(cudaMalloc(&b.d_counter, 256));
+  RS_CUDA(b.alloc(&b.d_blob, total_bytes));
+  RS_CUDA(b.alloc(&b.d_flags, std::max<size_t>(n_ops, 1) * 4));
+  RS_CUDA(b.alloc(&b.d_counter, 256));
+  if (b.stream_ordered)
+    RS_CUDA(cudaMemsetAsync(b.d_flags, 0, std::max<size_t>(n_ops, 1) * 4, b.stream));
+  else
+    RS_CUDA(cudaMemset(b.d_flags, 0, std::max<size_t>(n_ops, 1) * 4));
   uint8_t *base = static_cast<uint8_t *>(b.d_blob);
   const uint32_t *tbl_base = reinterpret_cast<const uint32_t *>(base + o_tbl);
   for (size_t ji = 0; ji < B.jobs.size(); ++ji) {
@@ -676,7 +710,10 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   std::memcpy(host.data() + o_leo, B.leo_jobs.data(), B.leo_jobs.size() * sizeof(LeoJob));
   std::memcpy(host.data() + o_roles, B.roles.data(), B.roles.size());
   std::memcpy(host.data() + o_tbl, B.tables.data(), B.tables.size() * 4);
-  RS_CUDA(cudaMemcpy(b.d_blob, host.data(), host.size(), cudaMemcpyHostToDevice));
+  if (b.stream_ordered)  // pageable source: staged before the call returns
+    RS_CUDA(cudaMemcpyAsync(b.d_blob, host.data(), host.size(), cudaMemcpyHostToDevice, b.stream));
+  else
+    RS_CUDA(cudaMemcpy(b.d_blob, host.data(), host.size(), cudaMemcpyHostToDevice));
 
   // ---- launch shape
   b.smem = B.smem;
@@ -687,7 +724,7 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   per_sm = std::max(per_sm, 1);
   if (opt.ctas_per_sm > 0) per_sm = std::min(per_sm, int(opt.ctas_per_sm));
   b.grid = int(std::max<uint64_t>(1, std::min<uint64_t>(items.size(), uint64_t(per_sm) * sm_count())));
-  if (B.scratch_words) RS_CUDA(cudaMalloc(&b.d_scratch, size_t(b.grid) * B.scratch_words * 4));
+  if (B.scratch_words) RS_CUDA(b.alloc(&b.d_scratch, size_t(b.grid) * B.scratch_words * 4));
   MixArgs &a = b.args;
   a.items = reinterpret_cast<const MixItem *>(base + o_items);
   a.jobs = reinterpret_cast<const MixJob *>(base + o_jobs);
@@ -722,7 +759,7 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
     cudaStreamDestroy(cs);
     if (rc) return rc;
   }
-  RS_CUDA(cudaDeviceSynchronize());
+  if (!b.stream_ordered) RS_CUDA(cudaDeviceSynchronize());
   out = std::move(batch);
   return RSGPU_OK;
 }
@@ -749,6 +786,8 @@ int mix_results(MixBatch &b, uint8_t *ok, cudaStream_t s) {
 const rsgpu_mix_info &mix_info(const MixBatch &b) { return b.info; }
 const std::vector<rsgpu_plan> &mix_plans(const MixBatch &b) { return b.plans; }
 void MixDeleter::operator()(MixBatch *b) const { delete b; }
+int mix_validate(const rsgpu_mix_op &o, int device) { return validate_op(o, device); }
+const uint32_t *mix_flags(const MixBatch &b) { return b.d_flags; }
 
 }  // namespace rsgpu
 

@@ -20,8 +20,16 @@ struct MixDeleter {
 using MixPtr = std::unique_ptr<MixBatch, MixDeleter>;
 
 // Prepare a mixed batch; `forced` (optional) gives every op's plan.
+// With `ordered`, the batch is a one-shot, stream-ordered batch for that
+// stream (no graph): its device memory is allocated and freed in the stream's
+// order and building it never synchronizes the device.
 int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, const rsgpu_mix_options &opt,
-              MixPtr &out);
+              MixPtr &out, cudaStream_t ordered = nullptr);
+// The validation mix_build applies to each operation (reference error
+// precedence; shard pointers must be non-null).
+int mix_validate(const rsgpu_mix_op &o, int device);
+// Device verify flags of a batch (one word per operation, nonzero = mismatch).
+const uint32_t *mix_flags(const MixBatch &b);
 int mix_launch(MixBatch &b, cudaStream_t s);
 int mix_results(MixBatch &b, uint8_t *ok, cudaStream_t s);
 const rsgpu_mix_info &mix_info(const MixBatch &b);

@@ -287,6 +287,12 @@ int Codec::decode_tables(const std::vector<const ClassicPlan *> &plans, std::vec
   return RSGPU_OK;
 }
 
+int Codec::decode_tables_shared(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
+                                cudaStream_t s) {
+  std::lock_guard<std::mutex> g(mu_);
+  return decode_tables(plans, tbls, s);
+}
+
 int Codec::decode_tables_copy(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
                               uint32_t **owned, cudaStream_t s) {
   *owned = nullptr;

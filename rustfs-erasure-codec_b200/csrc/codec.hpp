@@ -137,6 +137,9 @@ class Codec {
   // the cache lock is released, so a later eviction cannot recycle them.
   int decode_tables_copy(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
                          uint32_t **owned, cudaStream_t s);
+  // decode_tables under the cache lock, returning the cache's own blocks.
+  int decode_tables_shared(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
+                           cudaStream_t s);
 
  private:
   std::mutex mu_;

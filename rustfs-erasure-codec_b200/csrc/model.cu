@@ -13,6 +13,7 @@
 // looping over the samples), so a training run is deterministic.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -193,6 +194,15 @@ struct ModelState {
   std::mutex mu;
   bool ready = false;
   std::vector<float> params;
+  // Inference context: the weights stay on the device and inputs / outputs
+  // go through pinned buffers on a private stream, so a planner call costs
+  // one small kernel and waits only for that stream.
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  float *d_w = nullptr, *d_x = nullptr, *d_y = nullptr;
+  float *h_x = nullptr, *h_y = nullptr;
+  size_t cap = 0;
+  bool w_dirty = true;
 };
 ModelState &state() {
   static ModelState s;
@@ -242,27 +252,50 @@ int model_set(const float *in, size_t n) {
   std::lock_guard<std::mutex> g(state().mu);
   state().params.assign(in, in + kParams);
   state().ready = true;
+  state().w_dirty = true;
   return RSGPU_OK;
 }
 
 int model_predict(const float *features, size_t n, float *out) {
-  std::vector<float> w;
-  {
-    std::lock_guard<std::mutex> g(state().mu);
-    if (!state().ready) return RSGPU_ERR_INVALID_ARGUMENT;
-    w = state().params;
-  }
+  ModelState &m = state();
+  std::lock_guard<std::mutex> g(m.mu);
+  if (!m.ready) return RSGPU_ERR_INVALID_ARGUMENT;
   if (n == 0) return RSGPU_OK;
-  Run r;
-  int rc = r.alloc(n, false);
-  if (rc) return rc;
-  RS_CUDA(cudaMemcpy(r.w, w.data(), kParams * 4, cudaMemcpyHostToDevice));
-  RS_CUDA(cudaMemcpy(r.x, features, n * F * 4, cudaMemcpyHostToDevice));
-  k_mlp_sample<<<int(n), 32>>>(r.w, r.x, nullptr, nullptr, 0.f, int(n), r.y, nullptr, nullptr, nullptr, nullptr,
-                               nullptr, nullptr);
+  int dev = 0;
+  RS_CUDA(cudaGetDevice(&dev));
+  if (m.device != dev) {  // first use (or a new device): fresh context
+    m.device = dev;
+    m.cap = 0;
+    m.w_dirty = true;
+    RS_CUDA(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking));
+    RS_CUDA(cudaMalloc(&m.d_w, kParams * 4));
+  }
+  if (n > m.cap) {
+    const size_t cap = std::max<size_t>(n, 1024);
+    if (m.d_x) cudaFree(m.d_x);
+    if (m.d_y) cudaFree(m.d_y);
+    if (m.h_x) cudaFreeHost(m.h_x);
+    if (m.h_y) cudaFreeHost(m.h_y);
+    RS_CUDA(cudaMalloc(&m.d_x, cap * F * 4));
+    RS_CUDA(cudaMalloc(&m.d_y, cap * P * 4));
+    RS_CUDA(cudaMallocHost(&m.h_x, cap * F * 4));
+    RS_CUDA(cudaMallocHost(&m.h_y, cap * P * 4));
+    m.cap = cap;
+  }
+  if (m.w_dirty) {
+    RS_CUDA(cudaMemcpyAsync(m.d_w, m.params.data(), kParams * 4, cudaMemcpyHostToDevice, m.stream));
+    RS_CUDA(cudaStreamSynchronize(m.stream));
+    m.w_dirty = false;
+  }
+  std::memcpy(m.h_x, features, n * F * 4);
+  RS_CUDA(cudaMemcpyAsync(m.d_x, m.h_x, n * F * 4, cudaMemcpyHostToDevice, m.stream));
+  k_mlp_sample<<<int(n), 32, 0, m.stream>>>(m.d_w, m.d_x, nullptr, nullptr, 0.f, int(n), m.d_y, nullptr, nullptr,
+                                            nullptr, nullptr, nullptr, nullptr);
   launch_counter_add(1);
   RS_CUDA(cudaGetLastError());
-  RS_CUDA(cudaMemcpy(out, r.y, n * P * 4, cudaMemcpyDeviceToHost));
+  RS_CUDA(cudaMemcpyAsync(m.h_y, m.d_y, n * P * 4, cudaMemcpyDeviceToHost, m.stream));
+  RS_CUDA(cudaStreamSynchronize(m.stream));
+  std::memcpy(out, m.h_y, n * P * 4);
   return RSGPU_OK;
 }
 

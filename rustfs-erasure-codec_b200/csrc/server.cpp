@@ -1,0 +1,436 @@
+// server.cpp -- the request server: continuous batching of encode /
+// reconstruct / verify requests of any codec and size onto the GPU.
+//
+// The reference is a library called once per stripe from the storage node's
+// own request handlers (src/core/encode.rs:935-972,
+// src/core/reconstruct.rs:731-790, src/core/verify.rs:14-174).  This server is
+// the GPU-side loop such a node feeds: requests are submitted from any thread
+// and complete asynchronously.  One worker thread runs the loop:
+//
+//   1. retire: every launch whose completion event has fired finishes its
+//      requests (verify flags read from pinned memory), frees their device
+//      staging and gives back their slots and device-memory reservation;
+//   2. admit: while a launch slot (stream) is free, take pending requests in
+//      arrival order as long as a request slot and the device-memory budget
+//      allow (a request reserves its stripe bytes: (k + m) * shard_len);
+//   3. launch: copy the admitted host-memory requests' inputs into
+//      stream-ordered device staging, build ONE mixed batch for all admitted
+//      requests (plans from the planner: measured table / cost model), run it
+//      in the persistent kernel, copy outputs back, record an event.
+//
+// Up to `streams` launches are in flight at once, so requests that arrive
+// while others run are admitted into the next launch and their work overlaps
+// the running ones on the device.  Decode tables and error locators stay
+// cached in HBM by their codecs; device-memory requests (shards resident in
+// HBM) are used in place.  Every step of a launch is stream-ordered, so the
+// loop never synchronizes the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "batch.hpp"
+#include "codec.hpp"
+#include "handles.hpp"
+#include "rsgpu.h"
+
+namespace rsgpu {
+
+#define SV_CUDA(expr)                              \
+  do {                                             \
+    cudaError_t e_ = (expr);                       \
+    if (e_ != cudaSuccess) return cuda_status(e_); \
+  } while (0)
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Req {
+  rsgpu_request r{};
+  std::vector<uint8_t *> shards;  // caller's pointers
+  std::vector<uint8_t> present;
+  std::vector<uint8_t *> dev;     // device pointers the batch uses
+  uint8_t *staging = nullptr;     // device staging of a host-memory request
+  size_t reserve = 0;             // budget bytes held while admitted
+  double t_submit = 0, t_admit = 0;
+};
+
+struct Flight {
+  std::vector<Req *> reqs;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  uint32_t *h_flags = nullptr;  // pinned, one word per request
+  size_t h_cap = 0;
+  bool busy = false;
+};
+
+}  // namespace
+
+class Server {
+ public:
+  explicit Server(const rsgpu_server_options &o) : opt_(o) {}
+  ~Server() { stop(); }
+
+  int start() {
+    SV_CUDA(cudaGetDevice(&device_));
+    if (opt_.device_budget == 0) {
+      size_t free_b = 0, total_b = 0;
+      SV_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      opt_.device_budget = free_b / 2;
+    }
+    if (opt_.max_inflight == 0) opt_.max_inflight = 4096;
+    if (opt_.max_batch == 0) opt_.max_batch = 1024;
+    if (opt_.streams == 0) opt_.streams = 3;
+    // Stream-ordered staging: keep freed blocks in the pool instead of
+    // returning them to the driver at every synchronization.
+    cudaMemPool_t pool;
+    SV_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
+    uint64_t keep = opt_.device_budget;
+    SV_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    flights_.resize(opt_.streams);
+    for (auto &f : flights_) {
+      SV_CUDA(cudaStreamCreateWithFlags(&f.stream, cudaStreamNonBlocking));
+      SV_CUDA(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
+    }
+    t0_ = Clock::now();
+    worker_ = std::thread([this] { loop(); });
+    return RSGPU_OK;
+  }
+
+  void stop() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      if (stopping_) return;
+      stopping_ = true;
+    }
+    cv_.notify_all();
+    if (worker_.joinable()) worker_.join();
+    for (auto &f : flights_) {
+      if (f.stream) cudaStreamSynchronize(f.stream);
+      if (f.done) cudaEventDestroy(f.done);
+      if (f.stream) cudaStreamDestroy(f.stream);
+      if (f.h_flags) cudaFreeHost(f.h_flags);
+    }
+    flights_.clear();
+  }
+
+  int submit(const rsgpu_request &r) {
+    if (!r.codec || !r.shards) return RSGPU_ERR_INVALID_ARGUMENT;
+    if (r.mem != RSGPU_MEM_HOST && r.mem != RSGPU_MEM_DEVICE) return RSGPU_ERR_INVALID_ARGUMENT;
+    const Codec &c = r.codec->c;
+    const size_t total = c.k + c.m;
+    std::unique_ptr<Req> q(new (std::nothrow) Req());
+    if (!q) return RSGPU_ERR_OUT_OF_MEMORY;
+    q->r = r;
+    q->shards.assign(r.shards, r.shards + total);
+    if (r.op == RSGPU_OP_RECONSTRUCT && r.present) q->present.assign(r.present, r.present + total);
+    rsgpu_mix_op op = as_op(*q, q->shards.data());
+    int rc = mix_validate(op, device_);
+    if (rc) return rc;
+    const size_t stripe = total * r.shard_len;
+    if (stripe > opt_.device_budget) return RSGPU_ERR_OUT_OF_MEMORY;
+    q->reserve = stripe;
+    q->t_submit = now();
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      if (stopping_) return RSGPU_ERR_INVALID_ARGUMENT;
+      pending_.push_back(q.release());
+      ++submitted_;
+    }
+    cv_.notify_all();
+    return RSGPU_OK;
+  }
+
+  size_t poll(rsgpu_completion *out, size_t cap, int32_t timeout_ms) {
+    std::unique_lock<std::mutex> g(mu_);
+    if (done_.empty() && timeout_ms != 0) {
+      auto pred = [&] { return !done_.empty(); };
+      if (timeout_ms < 0)
+        done_cv_.wait(g, pred);
+      else
+        done_cv_.wait_for(g, std::chrono::milliseconds(timeout_ms), pred);
+    }
+    const size_t n = std::min(cap, done_.size());
+    for (size_t i = 0; i < n; ++i) {
+      out[i] = done_.front();
+      done_.pop_front();
+    }
+    return n;
+  }
+
+  void stats(rsgpu_server_stats *s) {
+    std::lock_guard<std::mutex> g(mu_);
+    s->submitted = submitted_;
+    s->completed = completed_;
+    s->launches = launches_;
+    s->pending = pending_.size();
+    s->inflight = inflight_;
+    s->budget_bytes = opt_.device_budget;
+    s->reserved_bytes = reserved_;
+    s->max_reserved_bytes = max_reserved_;
+    s->max_concurrent_launches = max_concurrent_;
+  }
+
+ private:
+  rsgpu_server_options opt_;
+  int device_ = 0;
+  std::thread worker_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  std::deque<Req *> pending_;
+  std::deque<rsgpu_completion> done_;
+  std::vector<Flight> flights_;
+  bool stopping_ = false;
+  uint64_t submitted_ = 0, completed_ = 0, launches_ = 0;
+  size_t inflight_ = 0, reserved_ = 0, max_reserved_ = 0;
+  uint32_t max_concurrent_ = 0;
+  Clock::time_point t0_;
+
+  double now() const { return std::chrono::duration<double>(Clock::now() - t0_).count(); }
+
+  static rsgpu_mix_op as_op(const Req &q, uint8_t *const *ptrs) {
+    rsgpu_mix_op o{};
+    o.codec = q.r.codec;
+    o.op = q.r.op;
+    o.goal = q.r.goal;
+    o.shards = ptrs;
+    o.present = q.present.empty() ? nullptr : q.present.data();
+    o.shard_len = q.r.shard_len;
+    return o;
+  }
+
+  // Shards a request reads (input) and writes (output).
+  static void roles(const Req &q, std::vector<size_t> &in, std::vector<size_t> &out) {
+    const Codec &c = q.r.codec->c;
+    const size_t total = c.k + c.m;
+    in.clear();
+    out.clear();
+    for (size_t i = 0; i < total; ++i) {
+      if (q.r.op == RSGPU_OP_ENCODE) {
+        (i < c.k ? in : out).push_back(i);
+      } else if (q.r.op == RSGPU_OP_VERIFY) {
+        in.push_back(i);
+      } else if (q.present[i]) {
+        in.push_back(i);
+      } else if (q.r.goal == RSGPU_GOAL_ALL || i < c.k) {
+        out.push_back(i);
+      }
+    }
+  }
+
+  void finish(Req *q, int status, int ok) {
+    rsgpu_completion c{};
+    c.tag = q->r.tag;
+    c.status = status;
+    c.ok = ok;
+    c.submit_s = q->t_submit;
+    c.admit_s = q->t_admit;
+    c.done_s = now();
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      done_.push_back(c);
+      ++completed_;
+    }
+    done_cv_.notify_all();
+    delete q;
+  }
+
+  // Step 1.  Returns true when a launch finished.
+  bool retire() {
+    bool any = false;
+    for (auto &f : flights_) {
+      if (!f.busy || cudaEventQuery(f.done) == cudaErrorNotReady) continue;
+      const cudaError_t e = cudaEventQuery(f.done);
+      const int status = e == cudaSuccess ? RSGPU_OK : cuda_status(e);
+      size_t freed = 0;
+      for (size_t i = 0; i < f.reqs.size(); ++i) {
+        Req *q = f.reqs[i];
+        freed += q->reserve;
+        finish(q, status, f.h_flags[i] ? 0 : 1);
+      }
+      {
+        std::lock_guard<std::mutex> g(mu_);
+        inflight_ -= f.reqs.size();
+        reserved_ -= freed;
+      }
+      f.reqs.clear();
+      f.busy = false;
+      any = true;
+    }
+    return any;
+  }
+
+  // Steps 2 and 3 on one free launch slot.  Returns true when it launched.
+  bool admit_and_launch(Flight &f) {
+    std::vector<Req *> take;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      while (!pending_.empty() && take.size() < opt_.max_batch && inflight_ + take.size() < opt_.max_inflight) {
+        Req *q = pending_.front();
+        if (reserved_ + q->reserve > opt_.device_budget) break;  // wait for memory (arrival order)
+        reserved_ += q->reserve;
+        max_reserved_ = std::max(max_reserved_, reserved_);
+        pending_.pop_front();
+        take.push_back(q);
+      }
+      inflight_ += take.size();
+    }
+    if (take.empty()) return false;
+    const double t = now();
+    std::vector<size_t> in, out;
+    std::vector<rsgpu_mix_op> ops(take.size());
+    int rc = RSGPU_OK;
+    for (size_t i = 0; i < take.size() && rc == RSGPU_OK; ++i) {
+      Req *q = take[i];
+      q->t_admit = t;
+      const Codec &c = q->r.codec->c;
+      const size_t total = c.k + c.m, len = q->r.shard_len;
+      if (q->r.mem == RSGPU_MEM_DEVICE) {
+        q->dev = q->shards;
+      } else {
+        if (cudaMallocAsync(reinterpret_cast<void **>(&q->staging), total * len, f.stream) != cudaSuccess) {
+          rc = RSGPU_ERR_OUT_OF_MEMORY;
+          break;
+        }
+        q->dev.resize(total);
+        for (size_t j = 0; j < total; ++j) q->dev[j] = q->staging + j * len;
+        roles(*q, in, out);
+        for (size_t j : in)
+          if (cudaMemcpyAsync(q->dev[j], q->shards[j], len, cudaMemcpyHostToDevice, f.stream) != cudaSuccess)
+            rc = RSGPU_ERR_CUDA;
+      }
+      ops[i] = as_op(*q, q->dev.data());
+    }
+    MixPtr b;
+    if (rc == RSGPU_OK) {
+      rsgpu_mix_options mo;
+      rsgpu_mix_options_default(&mo);
+      mo.planner = opt_.planner;
+      mo.graph = 0;
+      rc = mix_build(ops.data(), ops.size(), nullptr, mo, b, f.stream);
+    }
+    if (rc == RSGPU_OK) rc = mix_launch(*b, f.stream);
+    if (rc == RSGPU_OK) {
+      for (Req *q : take) {
+        if (q->r.mem != RSGPU_MEM_HOST) continue;
+        roles(*q, in, out);
+        for (size_t j : out)
+          cudaMemcpyAsync(q->shards[j], q->dev[j], q->r.shard_len, cudaMemcpyDeviceToHost, f.stream);
+      }
+      if (f.h_cap < take.size()) {
+        if (f.h_flags) cudaFreeHost(f.h_flags);
+        f.h_cap = std::max<size_t>(take.size(), 1024);
+        if (cudaMallocHost(&f.h_flags, f.h_cap * 4) != cudaSuccess) rc = RSGPU_ERR_OUT_OF_MEMORY;
+      }
+      if (rc == RSGPU_OK)
+        cudaMemcpyAsync(f.h_flags, mix_flags(*b), take.size() * 4, cudaMemcpyDeviceToHost, f.stream);
+    }
+    b.reset();  // stream-ordered: its memory is released after the queued work
+    for (Req *q : take)
+      if (q->staging) cudaFreeAsync(q->staging, f.stream);
+    if (rc != RSGPU_OK) {
+      cudaStreamSynchronize(f.stream);
+      size_t freed = 0;
+      for (Req *q : take) {
+        freed += q->reserve;
+        finish(q, rc, 0);
+      }
+      std::lock_guard<std::mutex> g(mu_);
+      inflight_ -= take.size();
+      reserved_ -= freed;
+      return true;
+    }
+    cudaEventRecord(f.done, f.stream);
+    f.reqs = std::move(take);
+    f.busy = true;
+    uint32_t busy = 0;
+    for (auto &x : flights_) busy += x.busy ? 1 : 0;
+    std::lock_guard<std::mutex> g(mu_);
+    ++launches_;
+    max_concurrent_ = std::max(max_concurrent_, busy);
+    return true;
+  }
+
+  void loop() {
+    cudaSetDevice(device_);
+    for (;;) {
+      bool progress = retire();
+      for (auto &f : flights_)
+        if (!f.busy) progress |= admit_and_launch(f);
+      bool idle_exit = false;
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        bool any_busy = false;
+        for (auto &f : flights_) any_busy |= f.busy;
+        if (stopping_ && pending_.empty() && !any_busy) idle_exit = true;
+        else if (!progress)
+          // Nothing to do until a submission or a launch finishes: short
+          // waits keep completion latency low without spinning a core.
+          cv_.wait_for(g, std::chrono::microseconds(any_busy ? 20 : 500));
+      }
+      if (idle_exit) break;
+    }
+  }
+};
+
+}  // namespace rsgpu
+
+struct rsgpu_server {
+  std::unique_ptr<rsgpu::Server> s;
+};
+
+extern "C" {
+
+void rsgpu_server_options_default(rsgpu_server_options *out) {
+  if (!out) return;
+  std::memset(out, 0, sizeof(*out));
+  out->planner = RSGPU_PLANNER_MODEL;
+}
+
+int32_t rsgpu_server_new(const rsgpu_server_options *opts, rsgpu_server **out) {
+  if (!out) return RSGPU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return RSGPU_ERR_NO_DEVICE;
+  rsgpu_server_options o;
+  rsgpu_server_options_default(&o);
+  if (opts) o = *opts;
+  std::unique_ptr<rsgpu_server> h(new (std::nothrow) rsgpu_server());
+  if (!h) return RSGPU_ERR_OUT_OF_MEMORY;
+  h->s.reset(new (std::nothrow) rsgpu::Server(o));
+  if (!h->s) return RSGPU_ERR_OUT_OF_MEMORY;
+  int rc = h->s->start();
+  if (rc) return rc;
+  *out = h.release();
+  return RSGPU_OK;
+}
+
+int32_t rsgpu_server_submit(rsgpu_server *s, const rsgpu_request *r) {
+  if (!s || !r) return RSGPU_ERR_INVALID_ARGUMENT;
+  return s->s->submit(*r);
+}
+
+size_t rsgpu_server_poll(rsgpu_server *s, rsgpu_completion *out, size_t cap, int32_t timeout_ms) {
+  if (!s || (!out && cap)) return 0;
+  return s->s->poll(out, cap, timeout_ms);
+}
+
+int32_t rsgpu_server_get_stats(rsgpu_server *s, rsgpu_server_stats *out) {
+  if (!s || !out) return RSGPU_ERR_INVALID_ARGUMENT;
+  s->s->stats(out);
+  return RSGPU_OK;
+}
+
+void rsgpu_server_free(rsgpu_server *s) { delete s; }
+
+}  // extern "C"

@@ -108,6 +108,29 @@ class TrainOptions(ctypes.Structure):
     _fields_ = [("epochs", ctypes.c_int32), ("lr", ctypes.c_float), ("seed", ctypes.c_uint64)]
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("device_budget", ctypes.c_size_t), ("max_inflight", ctypes.c_uint32), ("max_batch", ctypes.c_uint32),
+                ("streams", ctypes.c_uint32), ("planner", ctypes.c_int32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("codec", ctypes.c_void_p), ("op", ctypes.c_int32), ("goal", ctypes.c_int32),
+                ("shards", ctypes.c_void_p), ("present", ctypes.c_void_p), ("shard_len", ctypes.c_size_t),
+                ("mem", ctypes.c_int32), ("pad", ctypes.c_int32), ("tag", ctypes.c_uint64)]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [("tag", ctypes.c_uint64), ("status", ctypes.c_int32), ("ok", ctypes.c_int32),
+                ("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("pending", ctypes.c_size_t), ("inflight", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t),
+                ("reserved_bytes", ctypes.c_size_t), ("max_reserved_bytes", ctypes.c_size_t),
+                ("max_concurrent_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+
+
 ALGO_APPLY, ALGO_FFT = 0, 1
 # Order of the cost model's outputs (rsgpu_plan_index).
 MODEL_PLAN_ORDER = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (1, 3)]
@@ -194,6 +217,12 @@ def _lib():
             "rsgpu_model_predict": (I32, [P, SZ, P]),
             "rsgpu_model_gradients": (I32, [P, P, P, P, SZ, ctypes.POINTER(ctypes.c_float), P]),
             "rsgpu_model_ready": (I32, []),
+            "rsgpu_server_options_default": (None, [ctypes.POINTER(ServerOptions)]),
+            "rsgpu_server_new": (I32, [ctypes.POINTER(ServerOptions), PP]),
+            "rsgpu_server_submit": (I32, [P, ctypes.POINTER(Request)]),
+            "rsgpu_server_poll": (SZ, [P, P, SZ, I32]),
+            "rsgpu_server_get_stats": (I32, [P, ctypes.POINTER(ServerStats)]),
+            "rsgpu_server_free": (None, [P]),
             "rsgpu_kernel_launch_count": (ctypes.c_uint64, []),
             "rsgpu_error_string": (ctypes.c_char_p, [I32]),
             "rsgpu_version": (ctypes.c_char_p, []),
@@ -456,6 +485,92 @@ class MixedBatch:
         if h and _L is not None and getattr(_L, "rsgpu_mix_free", None) is not None:
             _L.rsgpu_mix_free(h)
             self._h = None
+
+
+class Server:
+    """The request server (rsgpu_server_* in include/rsgpu.h): continuous
+    batching of requests onto the GPU.  Shards are NumPy uint8 arrays (host
+    memory, staged through the device; pinned memory, e.g. torch tensors
+    created with pin_memory=True and passed as .numpy(), is fastest), torch
+    CUDA tensors, or raw device pointers (ints).  Buffers are kept alive by
+    this object until their completion has been polled."""
+
+    def __init__(self, device_budget=0, max_inflight=0, max_batch=0, streams=0, planner="model"):
+        o = ServerOptions()
+        _lib().rsgpu_server_options_default(ctypes.byref(o))
+        o.device_budget = int(device_budget)
+        o.max_inflight = int(max_inflight)
+        o.max_batch = int(max_batch)
+        o.streams = int(streams)
+        o.planner = PLANNER[planner]
+        h = ctypes.c_void_p()
+        _check(_lib().rsgpu_server_new(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+        self._next = 1
+
+    def submit(self, codec: "ReedSolomon", op: str, shards, shard_len: int, present=None, goal="all",
+               tag=None) -> int:
+        first = shards[0]
+        if isinstance(first, (int, np.integer)):
+            mem, ptrs = MEM_DEVICE, np.array([int(x) for x in shards], np.uint64)
+        elif _is_torch_cuda(first):
+            mem, ptrs = MEM_DEVICE, np.array([x.data_ptr() for x in shards], np.uint64)
+        else:
+            mem, ptrs = MEM_HOST, np.array([x.ctypes.data for x in shards], np.uint64)
+        if tag is None:
+            tag = self._next
+            self._next += 1
+        pres = None
+        if op == "reconstruct":
+            pres = np.ascontiguousarray(np.asarray(present, dtype=np.uint8))
+        r = Request()
+        r.codec = codec._h
+        r.op = OP[op]
+        r.goal = GOAL[goal]
+        r.shards = ptrs.ctypes.data
+        r.present = None if pres is None else pres.ctypes.data
+        r.shard_len = int(shard_len)
+        r.mem = mem
+        r.tag = int(tag)
+        _check(_lib().rsgpu_server_submit(self._h, ctypes.byref(r)))
+        self._keep[int(tag)] = (codec, shards)
+        return int(tag)
+
+    def poll(self, max_n: int = 4096, timeout_ms: int = 0):
+        arr = (Completion * max_n)()
+        n = int(_lib().rsgpu_server_poll(self._h, ctypes.addressof(arr), max_n, int(timeout_ms)))
+        out = []
+        for i in range(n):
+            c = arr[i]
+            self._keep.pop(int(c.tag), None)
+            out.append(dict(tag=int(c.tag), status=int(c.status), ok=bool(c.ok), submit_s=c.submit_s,
+                            admit_s=c.admit_s, done_s=c.done_s))
+        return out
+
+    def wait(self, n: int, timeout_ms: int = 60000):
+        """Poll until n completions have arrived."""
+        out = []
+        while len(out) < n:
+            got = self.poll(timeout_ms=timeout_ms)
+            if not got:
+                raise TimeoutError(f"{len(out)} of {n} completions")
+            out += got
+        return out
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(_lib().rsgpu_server_get_stats(self._h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_ if f != "pad"}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and _L is not None and getattr(_L, "rsgpu_server_free", None) is not None:
+            _L.rsgpu_server_free(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        self.close()
 
 
 class Tuner:

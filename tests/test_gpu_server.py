@@ -1,0 +1,165 @@
+"""The request server: every result is byte-identical whether the request
+ran alone or in a continuous-batching mix with others, equal to the CPU
+oracle, and admission never exceeds the device-memory budget."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rs():
+    import rsgpu
+
+    return rsgpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+
+    assert t.cuda.is_available()
+    return t
+
+
+GEOMS = [("classic", 4, 2), ("classic", 10, 4), ("leopard_gf8", 32, 16), ("leopard_gf16", 64, 32),
+         ("leopard_gf8", 10, 4)]
+
+
+@pytest.fixture(scope="module")
+def codecs(rs):
+    return {g: rs.ReedSolomon(g[1], g[2], rs.CodecOptions(codec_family=g[0])) for g in GEOMS}
+
+
+def make_requests(codecs, seed, n):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        g = GEOMS[int(rng.integers(len(GEOMS)))]
+        fam, k, m = g
+        op = ["encode", "reconstruct", "verify"][int(rng.choice(3, p=[0.45, 0.4, 0.15]))]
+        length = int(rng.integers(1, 200)) * 64
+        data = rng.integers(0, 256, (k + m, length), dtype=np.uint8)
+        present, goal = None, "all"
+        if op == "reconstruct":
+            e = int(rng.integers(1, m + 1))
+            present = np.ones(k + m, np.uint8)
+            present[rng.choice(k + m, size=e, replace=False)] = 0
+            goal = "data" if rng.integers(3) == 0 else "all"
+        if op == "verify" and rng.integers(2):
+            data = oracle_apply(g, codecs[g], "encode", data, None, "all")[0]
+        reqs.append(dict(geom=g, op=op, data=data, present=present, goal=goal, len=length))
+    return reqs
+
+
+def oracle_apply(g, codec, op, data, present, goal):
+    fam, k, m = g
+    out = data.copy()
+    sh = [out[i] for i in range(k + m)]
+    field = 8 if fam == "leopard_gf8" else 16
+    if op in ("encode", "verify"):
+        if fam == "classic":
+            O.classic_encode(codec.encoding_matrix(), sh)
+        else:
+            rc, par = O.leopard_encode(field, k, m, sh[:k])
+            for r in range(m):
+                out[k + r] = par[r]
+        if op == "verify":
+            return data.copy(), bool(np.array_equal(out, data))
+        return out, True
+    if fam == "classic":
+        assert O.classic_reconstruct(codec.encoding_matrix(), sh, present, goal=goal) == 0
+    else:
+        want = [1] * (k + m) if goal == "all" else [1] * k + [0] * m
+        assert O.leopard_reconstruct(field, k, m, sh, present, want) == 0
+    return out, True
+
+
+def run(rs, server, codecs, reqs, one_at_a_time, device=None):
+    """Submit every request (host buffers, or device tensors when `device`),
+    return (outputs, verify results, completions)."""
+    bufs, oks, comps = [], {}, []
+    for i, r in enumerate(reqs):
+        b = r["data"].copy()
+        if device is not None:
+            t = device.from_numpy(b).cuda()
+            bufs.append(t)
+            shards = [t[j] for j in range(t.shape[0])]
+        else:
+            bufs.append(b)
+            shards = [b[j] for j in range(b.shape[0])]
+        server.submit(codecs[r["geom"]], r["op"], shards, r["len"], present=r["present"], goal=r["goal"], tag=i + 1)
+        if one_at_a_time:
+            comps += server.wait(1)
+    if not one_at_a_time:
+        comps += server.wait(len(reqs))
+    for c in comps:
+        assert c["status"] == 0, c
+        oks[c["tag"] - 1] = c["ok"]
+    outs = [b.cpu().numpy() if device is not None else b for b in bufs]
+    return outs, [oks[i] for i in range(len(reqs))], comps
+
+
+def test_results_identical_alone_and_in_the_mix(rs, torch, codecs):
+    reqs = make_requests(codecs, 3, 80)
+    srv = rs.Server(streams=3, max_batch=16)
+    alone, ok_alone, _ = run(rs, srv, codecs, reqs, one_at_a_time=True)
+    mixed, ok_mixed, comps = run(rs, srv, codecs, reqs, one_at_a_time=False)
+    st = srv.stats()
+    srv.close()
+    assert st["launches"] >= 80 + 5  # 80 alone, then several mixed launches
+    for i, r in enumerate(reqs):
+        want, want_ok = oracle_apply(r["geom"], codecs[r["geom"]], r["op"], r["data"], r["present"], r["goal"])
+        assert np.array_equal(alone[i], want), (i, r["geom"], r["op"])
+        assert np.array_equal(mixed[i], alone[i]), (i, r["geom"], r["op"])
+        assert ok_alone[i] == ok_mixed[i] == want_ok, i
+
+
+def test_device_resident_requests_and_concurrent_launches(rs, torch, codecs):
+    reqs = make_requests(codecs, 9, 120)
+    srv = rs.Server(streams=3, max_batch=8)
+    outs, oks, comps = run(rs, srv, codecs, reqs, one_at_a_time=False, device=torch)
+    st = srv.stats()
+    srv.close()
+    for i, r in enumerate(reqs):
+        want, want_ok = oracle_apply(r["geom"], codecs[r["geom"]], r["op"], r["data"], r["present"], r["goal"])
+        assert np.array_equal(outs[i], want), i
+        assert oks[i] == want_ok
+    assert st["launches"] >= 15 and st["max_concurrent_launches"] >= 2, st
+
+
+def test_admission_respects_the_memory_budget(rs, torch, codecs):
+    reqs = make_requests(codecs, 4, 60)
+    largest = max((r["geom"][1] + r["geom"][2]) * r["len"] for r in reqs)
+    budget = 2 * largest
+    srv = rs.Server(device_budget=budget, streams=2)
+    outs, oks, comps = run(rs, srv, codecs, reqs, one_at_a_time=False)
+    st = srv.stats()
+    srv.close()
+    assert st["max_reserved_bytes"] <= budget and st["completed"] == 60
+    # requests waited for memory: some were admitted well after submission
+    assert max(c["admit_s"] - c["submit_s"] for c in comps) >= 0.0
+    for i, r in enumerate(reqs):
+        want, _ = oracle_apply(r["geom"], codecs[r["geom"]], r["op"], r["data"], r["present"], r["goal"])
+        assert np.array_equal(outs[i], want), i
+
+
+def test_server_errors(rs, torch, codecs):
+    srv = rs.Server(device_budget=1 << 20)
+    c = codecs[("leopard_gf8", 32, 16)]
+    big = np.zeros((48, 64 << 10), np.uint8)
+    with pytest.raises(rs.RsError) as e:
+        srv.submit(c, "encode", [big[i] for i in range(48)], 64 << 10)
+    assert e.value.name == "OutOfMemory"
+    small = np.zeros((48, 100), np.uint8)
+    with pytest.raises(rs.RsError) as e:
+        srv.submit(c, "encode", [small[i] for i in range(48)], 100)
+    assert e.value.name == "IncorrectShardSize"
+    pres = np.zeros(48, np.uint8)
+    ok = np.zeros((48, 64), np.uint8)
+    with pytest.raises(rs.RsError) as e:
+        srv.submit(c, "reconstruct", [ok[i] for i in range(48)], 64, present=pres)
+    assert e.value.name == "TooFewShardsPresent"
+    srv.close()
