@@ -61,6 +61,7 @@ enum {
   RSGPU_ERR_DEVICE_TIMEOUT = 103,
   RSGPU_ERR_NO_DEVICE = 104,
   RSGPU_ERR_SCRATCH_LIMIT = 105,
+  RSGPU_ERR_STREAM_IO = 106, /* a stream read/write callback failed (see rsgpu_stream_status) */
 };
 
 enum { RSGPU_MEM_HOST = 0, RSGPU_MEM_DEVICE = 1 };
@@ -216,6 +217,48 @@ int32_t rsgpu_batch_verify_result(rsgpu_batch *batch, uint8_t *ok, void *stream)
 /* Kernels one launch of this batch issues. */
 uint32_t rsgpu_batch_kernel_count(const rsgpu_batch *batch);
 void rsgpu_batch_free(rsgpu_batch *batch);
+
+/* ------------------------------------------------------------ block streaming */
+/* src/core/stream.rs:650-1000 (encode_stream, verify_stream,
+ * reconstruct_stream_from) over callbacks instead of Read / Write objects.
+ * A read callback fills up to `cap` bytes of shard `shard` and returns the
+ * count (0 at the end of that stream) or a negative error; the library retries
+ * short reads until the block is full or the stream ends.  A write callback
+ * writes all `len` bytes and returns >= 0, or a negative error.  Block size is
+ * clamped to [1 KiB, 16 MiB] (default 4 MiB).  Classic GF(2^8) codecs only;
+ * others get RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY, like the reference.  On an
+ * I/O failure the call returns RSGPU_ERR_STREAM_IO and `status` names the
+ * shard and the callback's code; codec errors return their code with the
+ * shard index in `status` (e.g. IncorrectShardSize for a short stream).
+ * Every output block before a failing block has been written. */
+typedef int64_t (*rsgpu_read_fn)(void *ctx, size_t shard, uint8_t *buf, size_t cap);
+typedef int64_t (*rsgpu_write_fn)(void *ctx, size_t shard, const uint8_t *buf, size_t len);
+typedef struct rsgpu_stream_options {
+  size_t block_size;
+} rsgpu_stream_options;
+enum { RSGPU_STREAM_OK = 0, RSGPU_STREAM_CODEC = 1, RSGPU_STREAM_READ = 2, RSGPU_STREAM_WRITE = 3 };
+typedef struct rsgpu_stream_status {
+  int32_t kind;       /* RSGPU_STREAM_* */
+  int32_t code;       /* codec: RSGPU_ERR_*; read / write: the callback's return value */
+  size_t shard_index;
+} rsgpu_stream_status;
+void rsgpu_stream_options_default(rsgpu_stream_options *out);
+/* encode_stream: n_data readers (data shards 0..k), n_parity writers (parity
+ * shards k..k+m, passed as shard indices k..k+m to the callback).  Shorter data
+ * streams are zero-padded to the block's longest one. */
+int32_t rsgpu_encode_stream(const rsgpu_codec *codec, size_t n_data, rsgpu_read_fn read, void *read_ctx,
+                            size_t n_parity, rsgpu_write_fn write, void *write_ctx, const rsgpu_stream_options *opts,
+                            rsgpu_stream_status *status);
+/* verify_stream: *ok = 1 when every block verifies. */
+int32_t rsgpu_verify_stream(const rsgpu_codec *codec, size_t n_shards, rsgpu_read_fn read, void *read_ctx,
+                            const rsgpu_stream_options *opts, int32_t *ok, rsgpu_stream_status *status);
+/* reconstruct_stream_from: has_reader[i] / has_writer[i] mark the present
+ * and the missing shards (exactly one of the two per index, else
+ * InvalidShardFlags); every missing shard is rebuilt and written. */
+int32_t rsgpu_reconstruct_stream_from(const rsgpu_codec *codec, size_t n_shards, const uint8_t *has_reader,
+                                      rsgpu_read_fn read, void *read_ctx, const uint8_t *has_writer,
+                                      rsgpu_write_fn write, void *write_ctx, const rsgpu_stream_options *opts,
+                                      rsgpu_stream_status *status);
 
 /* ------------------------------------------------------------ mixed batches */
 /* A mixed batch runs many stripes of different codecs (classic GF(2^8),

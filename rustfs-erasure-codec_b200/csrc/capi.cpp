@@ -621,6 +621,7 @@ const char *rsgpu_error_string(int32_t code) {
     case RSGPU_ERR_DEVICE_TIMEOUT: return "a bounded device wait expired";
     case RSGPU_ERR_NO_DEVICE: return "no CUDA device available";
     case RSGPU_ERR_SCRATCH_LIMIT: return "the code is wider than the no-allocation entry point's static buffers allow";
+    case RSGPU_ERR_STREAM_IO: return "a stream read or write callback failed";
     default: return "unknown error";
   }
 }

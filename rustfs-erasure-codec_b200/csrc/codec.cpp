@@ -423,6 +423,14 @@ int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len
   return RSGPU_OK;
 }
 
+int Codec::verify_dev_async(size_t n_stripes, uint8_t *const *shards, size_t len, uint32_t *flags_dev,
+                            cudaStream_t s) {
+  std::vector<JobDesc> jobs;
+  std::vector<const uint8_t *> ptrs;
+  encode_jobs(n_stripes, shards, jobs, ptrs, true);
+  return run_apply(jobs, ptrs, len, true, flags_dev, s);
+}
+
 int Codec::reconstruct_jobs(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, int goal,
                             const uint8_t *required, size_t n_required, std::vector<JobDesc> &jobs,
                             std::vector<const uint8_t *> &ptrs, cudaStream_t s, uint32_t **owned) {

@@ -23,9 +23,16 @@ namespace rsgpu {
 
 namespace {
 
-// Grid-stride loop of apply_tile over every (job, tile) of a launch.
-template <int NG, int V, int kBatch, int MIX, bool VERIFY>
-__global__ void __launch_bounds__(kApplyThreads) k_apply_vec(ApplyArgs a) {
+// L2 prefetch of `bytes` (a multiple of 16) at a 16-byte-aligned address.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Grid-stride loop of apply_tile over every (job, tile) of a launch.  With
+// PF, the CTA first asks L2 for the input columns of the tile it will take
+// next (one bulk prefetch per input shard), so those loads are L2 hits.
+template <int NG, int V, int kBatch, int MIX, bool VERIFY, bool PF = false, int MINB = 0>
+__global__ void __launch_bounds__(kApplyThreads, MINB ? MINB : ((NG == 1 && V <= 2) ? 4 : 1)) k_apply_vec(ApplyArgs a) {
   constexpr uint32_t kTile = kApplyThreads * kApplyVec * V;
   const uint32_t tiles_per_job = uint32_t((a.len + kTile - 1) / kTile);
   const uint32_t total = tiles_per_job * a.n_jobs;
@@ -33,6 +40,18 @@ __global__ void __launch_bounds__(kApplyThreads) k_apply_vec(ApplyArgs a) {
     const uint32_t job = t / tiles_per_job;
     const uint64_t tile_base = uint64_t(t - job * tiles_per_job) * kTile;
     const JobDesc d = a.jobs[job];
+    if (PF) {
+      const uint32_t t2 = t + gridDim.x;
+      if (t2 < total) {
+        const uint32_t job2 = t2 / tiles_per_job;
+        const uint64_t base2 = uint64_t(t2 - job2 * tiles_per_job) * kTile;
+        const JobDesc d2 = a.jobs[job2];
+        if (threadIdx.x < d2.n_in && base2 < d2.vec_len) {
+          const uint64_t left = d2.vec_len - base2;
+          prefetch_l2(a.ptrs[d2.ptr_off + threadIdx.x] + base2, uint32_t(left < kTile ? left : kTile));
+        }
+      }
+    }
     if (tile_base >= d.vec_len) continue;  // CTA-uniform
     apply_tile<NG, V, kBatch, MIX, VERIFY>(a.ptrs, a.flags, d, tile_base);
   }
@@ -180,14 +199,14 @@ int grid_for(const void *fn, int threads, size_t smem) {
   return sms * per_sm;
 }
 
-template <int NG, int V, int B, int MIX, bool VERIFY>
+template <int NG, int V, int B, int MIX, bool VERIFY, bool PF = false, int MINB = 0>
 void launch_vec(const ApplyArgs &a, cudaStream_t s) {
   static int grid_max = 0;
-  if (!grid_max) grid_max = grid_for((const void *)k_apply_vec<NG, V, B, MIX, VERIFY>, kApplyThreads, 0);
+  if (!grid_max) grid_max = grid_for((const void *)k_apply_vec<NG, V, B, MIX, VERIFY, PF, MINB>, kApplyThreads, 0);
   const uint64_t tile = uint64_t(kApplyThreads) * kApplyVec * V;
   const uint64_t tiles = ((a.len + tile - 1) / tile) * a.n_jobs;
   const int grid = int(tiles < uint64_t(grid_max) ? tiles : grid_max);
-  k_apply_vec<NG, V, B, MIX, VERIFY><<<grid, kApplyThreads, 0, s>>>(a);
+  k_apply_vec<NG, V, B, MIX, VERIFY, PF, MINB><<<grid, kApplyThreads, 0, s>>>(a);
 }
 
 // Tile variants the autotuner chooses from: (vectors per thread, inputs in
@@ -204,6 +223,15 @@ void launch_variant(const ApplyArgs &a, int variant, cudaStream_t s) {
     case 3: launch_vec<1, 1, 8, 1, VERIFY>(a, s); break;
     case 4: launch_vec<1, 1, 4, 1, VERIFY>(a, s); break;
     case 1: launch_vec<1, 2, 4, 1, VERIFY>(a, s); break;
+    case 5: launch_vec<1, 2, 4, 0, VERIFY, true>(a, s); break;
+    case 6: launch_vec<1, 1, 8, 0, VERIFY>(a, s); break;
+    case 7: launch_vec<1, 1, 8, 0, VERIFY, true>(a, s); break;
+    case 8: launch_vec<1, 4, 2, 0, VERIFY>(a, s); break;
+    case 9: launch_vec<1, 2, 2, 0, VERIFY, true>(a, s); break;
+    case 10: launch_vec<1, 1, 4, 0, VERIFY, false, 6>(a, s); break;
+    case 11: launch_vec<1, 1, 2, 0, VERIFY, false, 8>(a, s); break;
+    case 12: launch_vec<1, 2, 2, 0, VERIFY, false, 6>(a, s); break;
+    case 13: launch_vec<1, 1, 4, 0, VERIFY, false, 4>(a, s); break;
     default: launch_vec<1, 2, 4, 0, VERIFY>(a, s); break;
   }
 }

@@ -29,7 +29,7 @@ ERROR_NAMES = {
     9: "IncorrectShardSize", 10: "TooFewShardsPresent", 11: "EmptyShard", 12: "InvalidShardFlags",
     13: "InvalidIndex", 14: "InvalidCustomMatrix", 15: "UnsupportedCodecFamily",
     16: "UnsupportedLeopardPrototype", 100: "Cuda", 101: "OutOfMemory", 102: "InvalidArgument",
-    103: "DeviceTimeout", 104: "NoDevice", 105: "ScratchLimit",
+    103: "DeviceTimeout", 104: "NoDevice", 105: "ScratchLimit", 106: "StreamIo",
 }
 
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -131,6 +131,30 @@ class ServerStats(ctypes.Structure):
                 ("max_concurrent_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
 
 
+class StreamOptions(ctypes.Structure):
+    _fields_ = [("block_size", ctypes.c_size_t)]
+
+
+class StreamStatus(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("code", ctypes.c_int32), ("shard_index", ctypes.c_size_t)]
+
+
+_READFN = ctypes.CFUNCTYPE(ctypes.c_int64, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t)
+_WRITEFN = ctypes.CFUNCTYPE(ctypes.c_int64, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t)
+STREAM_KINDS = {1: "codec", 2: "read", 3: "write"}
+
+
+class StreamError(Exception):
+    """src/core/stream.rs StreamError: the shard index and what failed
+    (a codec error, or the reader's / writer's exception)."""
+
+    def __init__(self, kind: str, shard_index: int, error):
+        self.kind = kind
+        self.shard_index = int(shard_index)
+        self.error = error
+        super().__init__(f"{kind} error at shard {shard_index}: {error}")
+
+
 ALGO_APPLY, ALGO_FFT = 0, 1
 # Order of the cost model's outputs (rsgpu_plan_index).
 MODEL_PLAN_ORDER = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (1, 3)]
@@ -217,6 +241,13 @@ def _lib():
             "rsgpu_model_predict": (I32, [P, SZ, P]),
             "rsgpu_model_gradients": (I32, [P, P, P, P, SZ, ctypes.POINTER(ctypes.c_float), P]),
             "rsgpu_model_ready": (I32, []),
+            "rsgpu_stream_options_default": (None, [ctypes.POINTER(StreamOptions)]),
+            "rsgpu_encode_stream": (I32, [P, SZ, _READFN, P, SZ, _WRITEFN, P, ctypes.POINTER(StreamOptions),
+                                          ctypes.POINTER(StreamStatus)]),
+            "rsgpu_verify_stream": (I32, [P, SZ, _READFN, P, ctypes.POINTER(StreamOptions), ctypes.POINTER(I32),
+                                          ctypes.POINTER(StreamStatus)]),
+            "rsgpu_reconstruct_stream_from": (I32, [P, SZ, U8P, _READFN, P, U8P, _WRITEFN, P,
+                                                    ctypes.POINTER(StreamOptions), ctypes.POINTER(StreamStatus)]),
             "rsgpu_server_options_default": (None, [ctypes.POINTER(ServerOptions)]),
             "rsgpu_server_new": (I32, [ctypes.POINTER(ServerOptions), PP]),
             "rsgpu_server_submit": (I32, [P, ctypes.POINTER(Request)]),
@@ -485,6 +516,69 @@ class MixedBatch:
         if h and _L is not None and getattr(_L, "rsgpu_mix_free", None) is not None:
             _L.rsgpu_mix_free(h)
             self._h = None
+
+
+class _StreamIO:
+    """ctypes read / write callbacks over Python file-like objects; the first
+    exception a callback raises is kept and re-raised as a StreamError."""
+
+    def __init__(self, readers=None, writers=None):
+        self.readers = readers
+        self.writers = writers
+        self.exc = None
+
+        def read(ctx, shard, buf, cap):
+            try:
+                r = self.readers[shard]
+                mv = memoryview((ctypes.c_uint8 * cap).from_address(buf)).cast("B")
+                if hasattr(r, "readinto"):
+                    n = r.readinto(mv)
+                else:
+                    data = r.read(cap)
+                    n = len(data)
+                    mv[:n] = data
+                return int(n or 0)
+            except Exception as e:  # noqa: BLE001 - handed back to the caller
+                if self.exc is None:
+                    self.exc = (shard, e)
+                return -1
+
+        def write(ctx, shard, buf, n):
+            try:
+                data = bytes((ctypes.c_uint8 * n).from_address(buf)) if n else b""
+                w = self.writers[shard]
+                view = memoryview(data)
+                while view:
+                    k = w.write(view)
+                    if k is None:
+                        break
+                    if k == 0:
+                        raise OSError("write returned 0")
+                    view = view[k:]
+                return 0
+            except Exception as e:  # noqa: BLE001
+                if self.exc is None:
+                    self.exc = (shard, e)
+                return -1
+
+        self.read_fn = _READFN(read)
+        self.write_fn = _WRITEFN(write)
+
+    def check(self, rc, status):
+        if rc == 0:
+            return
+        kind = STREAM_KINDS.get(status.kind, "codec")
+        if rc == 106 and self.exc is not None:
+            raise StreamError(kind, self.exc[0], self.exc[1])
+        raise StreamError(kind, status.shard_index, RsError(rc))
+
+
+def _stream_opts(block_size):
+    o = StreamOptions()
+    _lib().rsgpu_stream_options_default(ctypes.byref(o))
+    if block_size is not None:
+        o.block_size = int(block_size)
+    return o
 
 
 class Server:
@@ -861,3 +955,57 @@ class ReedSolomon:
         ok = (ctypes.c_uint8 * max(1, len(stripes)))()
         _check(_lib().rsgpu_verify_batch(self._h, len(stripes), ptrs, lens[0] if flat else 0, ok, mem, stream))
         return [bool(v) for v in list(ok)[: len(stripes)]]
+
+    # ---- block streaming (src/core/stream.rs:650-1000)
+    def encode_stream(self, data, parity, block_size=None) -> None:
+        """Read data shards from `data` (file-like objects) block by block
+        and write the parity to `parity` (file-like objects)."""
+        k = self.data_shard_count()
+        io = _StreamIO(readers=list(data), writers={k + i: w for i, w in enumerate(parity)})
+        st = StreamStatus()
+        rc = _lib().rsgpu_encode_stream(self._h, len(data), io.read_fn, None, len(parity), io.write_fn, None,
+                                        ctypes.byref(_stream_opts(block_size)), ctypes.byref(st))
+        io.check(rc, st)
+
+    def verify_stream(self, shards, block_size=None) -> bool:
+        io = _StreamIO(readers=list(shards))
+        ok = I32()
+        st = StreamStatus()
+        rc = _lib().rsgpu_verify_stream(self._h, len(shards), io.read_fn, None, ctypes.byref(_stream_opts(block_size)),
+                                        ctypes.byref(ok), ctypes.byref(st))
+        io.check(rc, st)
+        return bool(ok.value)
+
+    def reconstruct_stream_from(self, readers, writers, block_size=None) -> None:
+        """readers[i] / writers[i]: a file-like object or None; exactly one of
+        the two per shard (present shards have a reader)."""
+        total = self.total_shard_count()
+        for cnt in (len(readers), len(writers)):
+            if cnt != total:
+                raise StreamError("codec", 0, RsError(1 if cnt < total else 2))
+        has_r = np.array([r is not None for r in readers], np.uint8)
+        has_w = np.array([w is not None for w in writers], np.uint8)
+        io = _StreamIO(readers=list(readers), writers=list(writers))
+        st = StreamStatus()
+        rc = _lib().rsgpu_reconstruct_stream_from(self._h, total, has_r.ctypes.data_as(U8P), io.read_fn, None,
+                                                  has_w.ctypes.data_as(U8P), io.write_fn, None,
+                                                  ctypes.byref(_stream_opts(block_size)), ctypes.byref(st))
+        io.check(rc, st)
+
+    def reconstruct_stream(self, shards, block_size=None) -> None:
+        """shards: one io.BytesIO per shard (src/core/stream.rs:839-946);
+        empty ones are missing and receive the recovered bytes, present ones
+        are read from the start."""
+        total = self.total_shard_count()
+        if len(shards) != total:
+            raise StreamError("codec", 0, RsError(1 if len(shards) < total else 2))
+        if self.codec_family() != "classic" or self.field != "gf8":
+            raise StreamError("codec", 0, RsError(15))
+        present = [len(s.getbuffer()) > 0 for s in shards]
+        if not any(present):
+            return
+        for s, p in zip(shards, present):
+            if p:
+                s.seek(0)
+        self.reconstruct_stream_from([s if p else None for s, p in zip(shards, present)],
+                                     [None if p else s for s, p in zip(shards, present)], block_size)
