@@ -123,6 +123,11 @@ int32_t rsgpu_codec_with_custom_matrix(size_t data_shards, size_t parity_shards,
 /* src/galois_16.rs:605 (galois_16::ReedSolomon::new): classic codec over the
  * GF((2^8)^2) tower field; shard lengths count bytes and must be even. */
 int32_t rsgpu_codec_new_gf16(size_t data_shards, size_t parity_shards, rsgpu_codec **out);
+/* galois_16::ReedSolomon::with_custom_matrix (src/core/codec.rs:546-615):
+ * rows = parity_shards x data_shards tower elements, 2 bytes each
+ * ([X coefficient, constant]). */
+int32_t rsgpu_codec_gf16_with_custom_matrix(size_t data_shards, size_t parity_shards, const uint8_t *rows,
+                                            rsgpu_codec **out);
 void rsgpu_codec_free(rsgpu_codec *codec);
 
 /* src/core/codec.rs:353-380 (data_shard_count, parity_shard_count, ...) */
@@ -217,6 +222,37 @@ int32_t rsgpu_batch_verify_result(rsgpu_batch *batch, uint8_t *ok, void *stream)
 /* Kernels one launch of this batch issues. */
 uint32_t rsgpu_batch_kernel_count(const rsgpu_batch *batch);
 void rsgpu_batch_free(rsgpu_batch *batch);
+
+/* ------------------------------------------------------------ incremental parity, layout, format */
+/* encode_single (src/core/encode.rs:889-909): data shard i_data's
+ * contribution to the parity; i_data == 0 overwrites the parity (c * d_0),
+ * later shards add to it, so calls for i = 0..k-1 in order give the full
+ * parity.  `shards` holds k + m buffers; only shard i_data is read and only
+ * the parity is written.  Leopard codecs: RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY. */
+int32_t rsgpu_encode_single(const rsgpu_codec *codec, size_t i_data, uint8_t *const *shards, const size_t *lens,
+                            size_t n, int32_t mem, void *stream);
+/* encode_single_sep (src/core/encode.rs:912-930). */
+int32_t rsgpu_encode_single_sep(const rsgpu_codec *codec, size_t i_data, const uint8_t *data, size_t data_len,
+                                uint8_t *const *parity, const size_t *parity_lens, size_t n_parity, int32_t mem,
+                                void *stream);
+/* update (src/core/encode.rs:1048-1120): parity += sum over changed data
+ * shards j of c[j] * (old_j + new_j); new_data[j] = NULL marks an unchanged
+ * shard (its new_lens entry is ignored). */
+int32_t rsgpu_update(const rsgpu_codec *codec, const uint8_t *const *old_data, const size_t *old_lens, size_t n_old,
+                     const uint8_t *const *new_data, const size_t *new_lens, size_t n_new, uint8_t *const *parity,
+                     const size_t *parity_lens, size_t n_parity, int32_t mem, void *stream);
+/* split / join (src/core/codec.rs:476-538), host memory, no device work:
+ * split writes k shards of rsgpu_split_shard_len(data_len) bytes back to back
+ * into `out` (zero-padded; Leopard rounds to a non-zero multiple of 64 bytes;
+ * lengths count bytes, 2 per element for galois_16); join concatenates the k
+ * data shards and keeps min(out_len, k * shard_len) bytes. */
+size_t rsgpu_split_shard_len(const rsgpu_codec *codec, size_t data_len);
+int32_t rsgpu_split(const rsgpu_codec *codec, const uint8_t *data, size_t data_len, uint8_t *out, size_t out_len);
+int32_t rsgpu_join(const rsgpu_codec *codec, const uint8_t *const *shards, const size_t *lens, size_t n,
+                   uint8_t *out, size_t out_len, size_t *written);
+/* EncodingFormat::stable_id_bytes (src/core/format.rs:168-220), version 1:
+ * *len = the identity's size; with out != NULL (cap >= *len) the bytes. */
+int32_t rsgpu_format_id(const rsgpu_codec *codec, uint8_t *out, size_t cap, size_t *len);
 
 /* ------------------------------------------------------------ block streaming */
 /* src/core/stream.rs:650-1000 (encode_stream, verify_stream,

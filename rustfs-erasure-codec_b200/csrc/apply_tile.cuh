@@ -91,7 +91,9 @@ __device__ __forceinline__ void st_stream(uint8_t *p, uint4 v) {
 // per pass over the inputs (outputs g*4 .. g*4+3).  MIX: 0 = every input uses
 // the 4+4 split, 1 = odd inputs use 5+3, 2 = all 5+3.  Must be called by all
 // kApplyThreads threads of the CTA (warp shuffles need full warps).
-template <int NG, int V, int kBatch, int MIX, bool VERIFY>
+// ACC: outputs accumulate (dst ^= product) instead of being overwritten,
+// for incremental parity updates (encode_single with i > 0, update).
+template <int NG, int V, int kBatch, int MIX, bool VERIFY, bool ACC = false>
 __device__ __forceinline__ void apply_tile(const uint8_t *const *ptrs, uint32_t *flags, const JobDesc &d,
                                            uint64_t tile_base) {
   const uint32_t lane = threadIdx.x & 31;
@@ -184,6 +186,9 @@ __device__ __forceinline__ void apply_tile(const uint8_t *const *ptrs, uint32_t 
             if (VERIFY) {
               uint4 e = ld_stream(dst);
               bad |= (e.x != o[r][0]) | (e.y != o[r][1]) | (e.z != o[r][2]) | (e.w != o[r][3]);
+            } else if (ACC) {
+              const uint4 e = *reinterpret_cast<const uint4 *>(dst);
+              st_stream(dst, make_uint4(o[r][0] ^ e.x, o[r][1] ^ e.y, o[r][2] ^ e.z, o[r][3] ^ e.w));
             } else {
               st_stream(dst, make_uint4(o[r][0], o[r][1], o[r][2], o[r][3]));
             }
@@ -201,7 +206,7 @@ __device__ __forceinline__ void apply_tile(const uint8_t *const *ptrs, uint32_t 
 // of job d: the path for shard tails that are not a multiple of 16 bytes, or
 // jobs whose pointers are not 16-byte aligned.  Returns true on a verify
 // mismatch.
-template <bool VERIFY>
+template <bool VERIFY, bool ACC = false>
 __device__ __forceinline__ bool apply_column(const uint8_t *const *ptrs, const JobDesc &d, uint64_t col) {
   const uint8_t *const *ptr = ptrs + d.ptr_off;
   bool bad = false;
@@ -217,6 +222,8 @@ __device__ __forceinline__ bool apply_column(const uint8_t *const *ptrs, const J
       const uint8_t b = uint8_t(acc >> (8 * r));
       if (VERIFY)
         bad |= (*dst != b);
+      else if (ACC)
+        *dst ^= b;
       else
         *dst = b;
     }

@@ -90,7 +90,7 @@ int new_codec(size_t k, size_t m, const rsgpu_options *opts, const uint8_t *cust
   if (k == 0) return RSGPU_ERR_TOO_FEW_DATA_SHARDS;
   if (m == 0) return RSGPU_ERR_TOO_FEW_PARITY_SHARDS;
   const size_t total = k + m;
-  if (custom) {
+  if (custom && field == RSGPU_FIELD_GF8) {
     if (total > 256) return RSGPU_ERR_TOO_MANY_SHARDS;
     if (o.codec_family != RSGPU_FAMILY_CLASSIC) return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY;
     o.matrix_mode = RSGPU_MATRIX_CUSTOM;
@@ -105,6 +105,7 @@ int new_codec(size_t k, size_t m, const rsgpu_options *opts, const uint8_t *cust
   } else {
     if (total > 65536) return RSGPU_ERR_TOO_MANY_SHARDS;
     if (o.codec_family != RSGPU_FAMILY_CLASSIC) return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY;
+    if (custom) o.matrix_mode = RSGPU_MATRIX_CUSTOM;
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RSGPU_ERR_NO_DEVICE;
@@ -118,7 +119,7 @@ int new_codec(size_t k, size_t m, const rsgpu_options *opts, const uint8_t *cust
   c.field = field;
   int rc;
   if (field == RSGPU_FIELD_GF16_TOWER)
-    rc = c.init_tower();
+    rc = c.init_tower(custom);
   else if (c.family == RSGPU_FAMILY_CLASSIC)
     rc = c.init_classic(custom);
   else
@@ -184,7 +185,8 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
     if (e != cudaSuccess) return rsgpu::cuda_status(e);
     dptr.resize(cnt * total);
     for (size_t i = 0; i < cnt * total; ++i) dptr[i] = stage + i * pitch;
-    // Inputs first so the codec's metadata upload (queued after) does not wait on them.
+    // Inputs are queued first; the job-table upload and the kernel follow them
+    // on the same stream.
     for (size_t sidx = 0; sidx < cnt; ++sidx) {
       const size_t st = base + sidx;
       for (size_t i = 0; i < total; ++i) {
@@ -289,6 +291,11 @@ int32_t rsgpu_codec_with_custom_matrix(size_t k, size_t m, const uint8_t *rows, 
 
 int32_t rsgpu_codec_new_gf16(size_t k, size_t m, rsgpu_codec **out) {
   return new_codec(k, m, nullptr, nullptr, RSGPU_FIELD_GF16_TOWER, out);
+}
+
+int32_t rsgpu_codec_gf16_with_custom_matrix(size_t k, size_t m, const uint8_t *rows, rsgpu_codec **out) {
+  if (!rows) return RSGPU_ERR_INVALID_CUSTOM_MATRIX;
+  return new_codec(k, m, nullptr, rows, RSGPU_FIELD_GF16_TOWER, out);
 }
 
 void rsgpu_codec_free(rsgpu_codec *h) {

@@ -322,7 +322,7 @@ void Codec::stats(rsgpu_cache_stats *out) {
 
 // ------------------------------------------------------------------ K1 submission
 int ApplyLaunch::build(std::vector<JobDesc> &jobs, const std::vector<const uint8_t *> &ptrs, size_t len, bool vfy,
-                       uint32_t *flags, cudaStream_t s, bool persistent) {
+                       uint32_t *flags, cudaStream_t s, bool persistent, bool accumulate) {
   verify = vfy;
   max_tail = 0;
   uint32_t max_out = 0;
@@ -355,6 +355,7 @@ int ApplyLaunch::build(std::vector<JobDesc> &jobs, const std::vector<const uint8
   args.n_jobs = uint32_t(jobs.size());
   args.max_out = max_out;
   args.any_vec = any_vec;
+  args.accumulate = accumulate ? 1 : 0;
   return RSGPU_OK;
 }
 
@@ -373,10 +374,10 @@ void ApplyLaunch::release(cudaStream_t s) {
 }
 
 int Codec::run_apply(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &ptrs, size_t len, bool verify,
-                     uint32_t *flags_dev, cudaStream_t s) {
+                     uint32_t *flags_dev, cudaStream_t s, bool accumulate) {
   if (jobs.empty()) return RSGPU_OK;
   ApplyLaunch l;
-  int rc = l.build(jobs, ptrs, len, verify, flags_dev, s, false);
+  int rc = l.build(jobs, ptrs, len, verify, flags_dev, s, false, accumulate);
   if (rc) return rc;
   rc = l.launch(s);
   l.release(s);
@@ -421,6 +422,30 @@ int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len
   RS_CUDA(cudaStreamSynchronize(s));
   for (size_t i = 0; i < n_stripes; ++i) ok_host[i] = f[i] ? 0 : 1;
   return RSGPU_OK;
+}
+
+int Codec::apply_parity_columns(const std::vector<const uint8_t *> &inputs, const std::vector<size_t> &cols,
+                                uint8_t *const *parity, size_t len, bool accumulate, cudaStream_t s) {
+  if (inputs.empty()) return RSGPU_OK;
+  const size_t n_in = inputs.size();
+  std::vector<uint8_t> rows(m * n_in);
+  for (size_t r = 0; r < m; ++r)
+    for (size_t j = 0; j < n_in; ++j) rows[r * n_in + j] = matrix[(k + r) * k + cols[j]];
+  std::vector<uint32_t> tbl(packed_table_words(m, n_in));
+  pack_tables(rows.data(), m, n_in, tbl.data());
+  void *d_tbl = nullptr;
+  int rc = upload(tbl.data(), tbl.size() * 4, &d_tbl, s);
+  if (rc) return rc;
+  std::vector<JobDesc> jobs(1);
+  jobs[0].ptr_off = 0;
+  jobs[0].n_in = uint16_t(n_in);
+  jobs[0].n_out = uint16_t(m);
+  jobs[0].tbl = static_cast<const uint32_t *>(d_tbl);
+  std::vector<const uint8_t *> ptrs(inputs);
+  for (size_t r = 0; r < m; ++r) ptrs.push_back(parity[r]);
+  rc = run_apply(jobs, ptrs, len, false, nullptr, s, accumulate);
+  RS_CUDA(cudaFreeAsync(d_tbl, s));
+  return rc;
 }
 
 int Codec::verify_dev_async(size_t n_stripes, uint8_t *const *shards, size_t len, uint32_t *flags_dev,

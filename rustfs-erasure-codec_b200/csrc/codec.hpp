@@ -89,7 +89,7 @@ struct ApplyLaunch {
   uint64_t max_tail = 0;
   bool verify = false;
   int build(std::vector<JobDesc> &jobs, const std::vector<const uint8_t *> &ptrs, size_t len, bool verify,
-            uint32_t *flags, cudaStream_t s, bool persistent);
+            uint32_t *flags, cudaStream_t s, bool persistent, bool accumulate = false);
   int launch(cudaStream_t s) const;
   void release(cudaStream_t s);
 };
@@ -112,7 +112,7 @@ class Codec {
 
   ~Codec();
   int init_classic(const uint8_t *custom_rows);
-  int init_tower();
+  int init_tower(const uint8_t *custom_rows);
   int init_leopard();
 
   // ---- validation (reference error precedence)
@@ -128,6 +128,13 @@ class Codec {
   int verify_dev_async(size_t n_stripes, uint8_t *const *shards, size_t len, uint32_t *flags_dev, cudaStream_t s);
   int reconstruct_dev(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
                       int goal, const uint8_t *required, size_t n_required, cudaStream_t s);
+
+  // Incremental parity (src/core/encode.rs:890-930, 1048-1120): for one
+  // stripe, parity_r (+)= sum_j c[r][j] * in[j] over the given inputs, where
+  // c[r][j] = encoding matrix (k + r, cols[j]); `accumulate` adds into the
+  // parity instead of overwriting it.  Device pointers.
+  int apply_parity_columns(const std::vector<const uint8_t *> &inputs, const std::vector<size_t> &cols,
+                           uint8_t *const *parity, size_t len, bool accumulate, cudaStream_t s);
 
   // Decode tables for a set of plans, building missing entries on the GPU (K3).
   int decode_tables(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
@@ -152,7 +159,7 @@ class Codec {
   rsgpu_cache_stats stats_{};
   size_t capacity_ = 0;
   int run_apply(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &ptrs, size_t len, bool verify,
-                uint32_t *flags_dev, cudaStream_t s);
+                uint32_t *flags_dev, cudaStream_t s, bool accumulate = false);
 
  public:
   // Job lists for the three classic operations over device pointers.  With

@@ -31,7 +31,7 @@ __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
 // Grid-stride loop of apply_tile over every (job, tile) of a launch.  With
 // PF, the CTA first asks L2 for the input columns of the tile it will take
 // next (one bulk prefetch per input shard), so those loads are L2 hits.
-template <int NG, int V, int kBatch, int MIX, bool VERIFY, bool PF = false, int MINB = 0>
+template <int NG, int V, int kBatch, int MIX, bool VERIFY, bool PF = false, int MINB = 0, bool ACC = false>
 __global__ void __launch_bounds__(kApplyThreads, MINB ? MINB : ((NG == 1 && V <= 2) ? 4 : 1)) k_apply_vec(ApplyArgs a) {
   constexpr uint32_t kTile = kApplyThreads * kApplyVec * V;
   const uint32_t tiles_per_job = uint32_t((a.len + kTile - 1) / kTile);
@@ -53,13 +53,13 @@ __global__ void __launch_bounds__(kApplyThreads, MINB ? MINB : ((NG == 1 && V <=
       }
     }
     if (tile_base >= d.vec_len) continue;  // CTA-uniform
-    apply_tile<NG, V, kBatch, MIX, VERIFY>(a.ptrs, a.flags, d, tile_base);
+    apply_tile<NG, V, kBatch, MIX, VERIFY, ACC>(a.ptrs, a.flags, d, tile_base);
   }
 }
 
 // Byte-granular path for the columns past each job's vec_len.  One thread per
 // byte column.
-template <bool VERIFY>
+template <bool VERIFY, bool ACC = false>
 __global__ void k_apply_tail(ApplyArgs a, uint64_t max_tail) {
   const uint64_t n = max_tail * a.n_jobs;
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
@@ -68,7 +68,7 @@ __global__ void k_apply_tail(ApplyArgs a, uint64_t max_tail) {
     const JobDesc d = a.jobs[job];
     const uint64_t col = d.vec_len + (i - uint64_t(job) * max_tail);
     if (col >= a.len) continue;
-    if (apply_column<VERIFY>(a.ptrs, d, col) && VERIFY) atomicOr(a.flags + d.flag_idx, 1u);
+    if (apply_column<VERIFY, ACC>(a.ptrs, d, col) && VERIFY) atomicOr(a.flags + d.flag_idx, 1u);
   }
 }
 
@@ -199,14 +199,15 @@ int grid_for(const void *fn, int threads, size_t smem) {
   return sms * per_sm;
 }
 
-template <int NG, int V, int B, int MIX, bool VERIFY, bool PF = false, int MINB = 0>
+template <int NG, int V, int B, int MIX, bool VERIFY, bool PF = false, int MINB = 0, bool ACC = false>
 void launch_vec(const ApplyArgs &a, cudaStream_t s) {
   static int grid_max = 0;
-  if (!grid_max) grid_max = grid_for((const void *)k_apply_vec<NG, V, B, MIX, VERIFY, PF, MINB>, kApplyThreads, 0);
+  if (!grid_max)
+    grid_max = grid_for((const void *)k_apply_vec<NG, V, B, MIX, VERIFY, PF, MINB, ACC>, kApplyThreads, 0);
   const uint64_t tile = uint64_t(kApplyThreads) * kApplyVec * V;
   const uint64_t tiles = ((a.len + tile - 1) / tile) * a.n_jobs;
   const int grid = int(tiles < uint64_t(grid_max) ? tiles : grid_max);
-  k_apply_vec<NG, V, B, MIX, VERIFY, PF, MINB><<<grid, kApplyThreads, 0, s>>>(a);
+  k_apply_vec<NG, V, B, MIX, VERIFY, PF, MINB, ACC><<<grid, kApplyThreads, 0, s>>>(a);
 }
 
 // Tile variants the autotuner chooses from: (vectors per thread, inputs in
@@ -250,7 +251,9 @@ cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cud
   if (a.n_jobs == 0) return cudaSuccess;
   uint64_t launches = 0;
   if (a.any_vec && a.len >= 16) {
-    if (verify)
+    if (a.accumulate)
+      launch_vec<1, 2, 4, 0, false, false, 0, true>(a, s);
+    else if (verify)
       launch_variant<true>(a, apply_variant(), s);
     else
       launch_variant<false>(a, apply_variant(), s);
@@ -261,7 +264,9 @@ cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cud
     const int threads = 256;
     const uint64_t want = (n + threads - 1) / threads;
     const int grid = int(want < 148 * 16 ? want : 148 * 16);
-    if (verify)
+    if (a.accumulate)
+      k_apply_tail<false, true><<<grid, threads, 0, s>>>(a, max_tail);
+    else if (verify)
       k_apply_tail<true><<<grid, threads, 0, s>>>(a, max_tail);
     else
       k_apply_tail<false><<<grid, threads, 0, s>>>(a, max_tail);

@@ -16,6 +16,7 @@ struct ApplyArgs {
   uint32_t n_jobs;
   uint32_t max_out;             // largest n_out over the jobs
   int any_vec;                  // some job has vec_len > 0
+  int accumulate;               // outputs ^= products (incremental parity update)
 };
 cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cudaStream_t s);
 // K1 tile variant (threads x vectors-per-thread x inputs-in-flight); the

@@ -70,6 +70,9 @@ int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, s
                          cudaStream_t s);
 
 int tower_encode(Codec &c, size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s);
+// Tower-field incremental parity: parity_r (+)= sum_j t[k + r][cols[j]] * inputs[j] (one stripe).
+int tower_apply_columns(Codec &c, const std::vector<const uint8_t *> &inputs, const std::vector<size_t> &cols,
+                        uint8_t *const *parity, size_t len, bool accumulate, cudaStream_t s);
 int tower_verify(Codec &c, size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok,
                  cudaStream_t s);
 int tower_reconstruct(Codec &c, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,

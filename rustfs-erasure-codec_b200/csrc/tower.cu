@@ -92,6 +92,9 @@ __global__ void __launch_bounds__(256) k_apply_tower(ApplyArgs a) {
           if (VERIFY) {
             uint4 e = *reinterpret_cast<const uint4 *>(dst);
             bad |= (e.x != o.x) | (e.y != o.y) | (e.z != o.z) | (e.w != o.w);
+          } else if (a.accumulate) {  // incremental parity update
+            const uint4 e = *reinterpret_cast<const uint4 *>(dst);
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(o.x ^ e.x, o.y ^ e.y, o.z ^ e.z, o.w ^ e.w);
           } else {
             *reinterpret_cast<uint4 *>(dst) = o;
           }
@@ -101,6 +104,8 @@ __global__ void __launch_bounds__(256) k_apply_tower(ApplyArgs a) {
           for (int i = 0; i < 16 && col + i < a.len; ++i) {
             if (VERIFY)
               bad |= dst[i] != b[i];
+            else if (a.accumulate)
+              dst[i] ^= b[i];
             else
               dst[i] = b[i];
           }
@@ -150,10 +155,20 @@ struct TowerState {
 
 static TowerState *tower_state(const Codec &c) { return c.tower.get(); }
 
-int Codec::init_tower() {
+int Codec::init_tower(const uint8_t *custom_rows) {
   RS_CUDA(cudaGetDevice(&device));
-  int rc = build_tower_matrix(k, m, tmatrix);
-  if (rc) return rc;
+  if (custom_rows) {
+    // src/core/codec.rs:546-615 (with_custom_matrix): identity on top, the
+    // caller's m x k rows ([X coefficient, constant] per element) below.
+    tmatrix.assign((k + m) * k, T16{0, 0});
+    for (size_t i = 0; i < k; ++i) tmatrix[i * k + i] = T16{0, 1};
+    for (size_t r = 0; r < m; ++r)
+      for (size_t j = 0; j < k; ++j)
+        tmatrix[(k + r) * k + j] = T16{custom_rows[2 * (r * k + j)], custom_rows[2 * (r * k + j) + 1]};
+  } else {
+    int rc = build_tower_matrix(k, m, tmatrix);
+    if (rc) return rc;
+  }
   auto st = std::make_shared<TowerState>();
   std::vector<uint32_t> packed(tower_words(m, k));
   pack_tower(&tmatrix[k * k], m, k, packed.data());
@@ -164,7 +179,7 @@ int Codec::init_tower() {
 }
 
 static int launch_tower(const std::vector<JobDesc> &jobs, const std::vector<const uint8_t *> &ptrs, size_t len,
-                        bool verify, uint32_t *flags, cudaStream_t s) {
+                        bool verify, uint32_t *flags, cudaStream_t s, bool accumulate = false) {
   if (jobs.empty()) return RSGPU_OK;
   std::vector<JobDesc> js = jobs;
   for (auto &j : js) {
@@ -186,6 +201,7 @@ static int launch_tower(const std::vector<JobDesc> &jobs, const std::vector<cons
   a.flags = flags;
   a.len = len;
   a.n_jobs = uint32_t(js.size());
+  a.accumulate = accumulate ? 1 : 0;
   const uint64_t tiles = ((len + 4095) / 4096) * js.size();
   const int grid = int(std::min<uint64_t>(tiles, 148 * 8));
   if (verify)
@@ -197,6 +213,29 @@ static int launch_tower(const std::vector<JobDesc> &jobs, const std::vector<cons
   RS_CUDA(cudaStreamSynchronize(s));
   cudaFree(d);
   return RSGPU_OK;
+}
+
+int tower_apply_columns(Codec &c, const std::vector<const uint8_t *> &inputs, const std::vector<size_t> &cols,
+                        uint8_t *const *parity, size_t len, bool accumulate, cudaStream_t s) {
+  if (inputs.empty()) return RSGPU_OK;
+  const size_t k = c.k, m = c.m, n_in = inputs.size();
+  std::vector<T16> rows(m * n_in);
+  for (size_t r = 0; r < m; ++r)
+    for (size_t j = 0; j < n_in; ++j) rows[r * n_in + j] = c.tmatrix[(k + r) * k + cols[j]];
+  std::vector<uint32_t> packed(tower_words(m, n_in));
+  pack_tower(rows.data(), m, n_in, packed.data());
+  uint32_t *d_tbl = nullptr;
+  RS_CUDA(cudaMalloc(&d_tbl, packed.size() * 4));
+  RS_CUDA(cudaMemcpy(d_tbl, packed.data(), packed.size() * 4, cudaMemcpyHostToDevice));
+  std::vector<JobDesc> jobs(1);
+  jobs[0].n_in = uint16_t(n_in);
+  jobs[0].n_out = uint16_t(m);
+  jobs[0].tbl = d_tbl;
+  std::vector<const uint8_t *> ptrs(inputs);
+  for (size_t r = 0; r < m; ++r) ptrs.push_back(parity[r]);
+  int rc = launch_tower(jobs, ptrs, len, false, nullptr, s, accumulate);
+  cudaFree(d_tbl);
+  return rc;
 }
 
 int tower_encode(Codec &c, size_t n, uint8_t *const *shards, size_t len, cudaStream_t s) {

@@ -189,6 +189,14 @@ def _lib():
             "rsgpu_codec_new": (I32, [SZ, SZ, ctypes.POINTER(_Options), PP]),
             "rsgpu_codec_with_custom_matrix": (I32, [SZ, SZ, U8P, ctypes.POINTER(_Options), PP]),
             "rsgpu_codec_new_gf16": (I32, [SZ, SZ, PP]),
+            "rsgpu_codec_gf16_with_custom_matrix": (I32, [SZ, SZ, U8P, PP]),
+            "rsgpu_encode_single": (I32, [P, SZ, PP, SZP, SZ, I32, P]),
+            "rsgpu_encode_single_sep": (I32, [P, SZ, P, SZ, PP, SZP, SZ, I32, P]),
+            "rsgpu_update": (I32, [P, PP, SZP, SZ, PP, SZP, SZ, PP, SZP, SZ, I32, P]),
+            "rsgpu_split_shard_len": (SZ, [P, SZ]),
+            "rsgpu_split": (I32, [P, P, SZ, P, SZ]),
+            "rsgpu_join": (I32, [P, PP, SZP, SZ, P, SZ, SZP]),
+            "rsgpu_format_id": (I32, [P, P, SZ, SZP]),
             "rsgpu_codec_free": (None, [P]),
             "rsgpu_data_shard_count": (SZ, [P]),
             "rsgpu_parity_shard_count": (SZ, [P]),
@@ -788,7 +796,11 @@ class ReedSolomon:
                  *, field: str = "gf8", _custom=None):
         h = ctypes.c_void_p()
         L = _lib()
-        if field == "gf16":
+        if field == "gf16" and _custom is not None:
+            rows = np.ascontiguousarray(np.array(_custom, np.uint8).reshape(-1))
+            _check(L.rsgpu_codec_gf16_with_custom_matrix(data_shards, parity_shards, rows.ctypes.data_as(U8P),
+                                                         ctypes.byref(h)))
+        elif field == "gf16":
             _check(L.rsgpu_codec_new_gf16(data_shards, parity_shards, ctypes.byref(h)))
         elif _custom is not None:
             o = (options or CodecOptions())._c()
@@ -813,8 +825,11 @@ class ReedSolomon:
 
     # src/core/codec.rs:546-615
     @classmethod
-    def with_custom_matrix(cls, data_shards, parity_shards, rows, options: Optional[CodecOptions] = None):
-        return cls(data_shards, parity_shards, options, _custom=rows)
+    def with_custom_matrix(cls, data_shards, parity_shards, rows, options: Optional[CodecOptions] = None,
+                           field: str = "gf8"):
+        """rows: parity_shards x data_shards coefficients (galois_16: pairs
+        [X coefficient, constant])."""
+        return cls(data_shards, parity_shards, options, field=field, _custom=rows)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -1009,3 +1024,122 @@ class ReedSolomon:
                 s.seek(0)
         self.reconstruct_stream_from([s if p else None for s, p in zip(shards, present)],
                                      [None if p else s for s, p in zip(shards, present)], block_size)
+
+    # ---- incremental parity (src/core/encode.rs:889-930, 1048-1120)
+    def encode_single(self, i_data: int, shards: Sequence) -> None:
+        mem, ptrs, lens, stream, keep = _buffer_info(shards)
+        _check(_lib().rsgpu_encode_single(self._h, int(i_data), ptrs, lens, len(shards), mem, stream))
+
+    def encode_single_sep(self, i_data: int, data, parity: Sequence) -> None:
+        mem, ptrs, lens, stream, keep = _buffer_info(list(parity) + [data])
+        n = len(parity)
+        _check(_lib().rsgpu_encode_single_sep(self._h, int(i_data), ptrs[n], lens[n], ptrs, lens, n, mem, stream))
+
+    def update(self, old_data: Sequence, new_data: Sequence, parity: Sequence) -> None:
+        """new_data[j] is None for an unchanged data shard."""
+        changed = [x for x in new_data if x is not None]
+        mem, ptrs, lens, stream, keep = _buffer_info(list(old_data) + changed + list(parity))
+        no, nc, npar = len(old_data), len(changed), len(parity)
+        new_ptrs = (ctypes.c_void_p * max(1, len(new_data)))()
+        new_lens = (ctypes.c_size_t * max(1, len(new_data)))()
+        c = 0
+        for j, x in enumerate(new_data):
+            if x is not None:
+                new_ptrs[j] = ptrs[no + c]
+                new_lens[j] = lens[no + c]
+                c += 1
+        par_ptrs = (ctypes.c_void_p * max(1, npar))(*[ptrs[no + nc + r] for r in range(npar)])
+        par_lens = (ctypes.c_size_t * max(1, npar))(*[lens[no + nc + r] for r in range(npar)])
+        _check(_lib().rsgpu_update(self._h, ptrs, lens, no, new_ptrs, new_lens, len(new_data), par_ptrs, par_lens,
+                                   npar, mem, stream))
+
+    # ---- layout and format (src/core/codec.rs:476-538, src/core/format.rs:168-220)
+    def split(self, data) -> List[np.ndarray]:
+        """Data shards of `data` (bytes / uint8 array), zero-padded."""
+        buf = np.frombuffer(bytes(data), np.uint8) if not isinstance(data, np.ndarray) else np.ascontiguousarray(data)
+        sl = int(_lib().rsgpu_split_shard_len(self._h, buf.size))
+        k = self.data_shard_count()
+        out = np.zeros(k * sl, np.uint8)
+        _check(_lib().rsgpu_split(self._h, buf.ctypes.data if buf.size else None, buf.size,
+                                  out.ctypes.data if out.size else None, out.size))
+        return [out[i * sl:(i + 1) * sl] for i in range(k)]
+
+    def join(self, shards: Sequence, out_len: int) -> bytes:
+        arrs = [np.ascontiguousarray(np.asarray(s, np.uint8)) for s in shards]
+        ptrs = (ctypes.c_void_p * max(1, len(arrs)))(*[a.ctypes.data for a in arrs])
+        lens = (ctypes.c_size_t * max(1, len(arrs)))(*[a.size for a in arrs])
+        cap = min(out_len, sum(a.size for a in arrs))
+        out = np.zeros(max(cap, 1), np.uint8)
+        wrote = ctypes.c_size_t()
+        _check(_lib().rsgpu_join(self._h, ptrs, lens, len(arrs), out.ctypes.data, out_len, ctypes.byref(wrote)))
+        return out[: wrote.value].tobytes()
+
+    def stable_id_bytes(self) -> bytes:
+        n = ctypes.c_size_t()
+        _check(_lib().rsgpu_format_id(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, np.uint8)
+        _check(_lib().rsgpu_format_id(self._h, out.ctypes.data, out.size, ctypes.byref(n)))
+        return out.tobytes()
+
+
+class SBSError(Exception):
+    """src/errors.rs SBSError: TooManyCalls, LeftoverShards or an RSError."""
+
+    def __init__(self, kind: str, rs_error: Optional[RsError] = None):
+        self.kind = kind
+        self.rs_error = rs_error
+        super().__init__(kind if rs_error is None else f"{kind}: {rs_error}")
+
+
+class ShardByShard:
+    """src/core/shard_by_shard.rs: encode the data shards one at a time."""
+
+    def __init__(self, codec: ReedSolomon):
+        self.codec = codec
+        self.cur_input = 0
+
+    def parity_ready(self) -> bool:
+        return self.cur_input == self.codec.data_shard_count()
+
+    def reset(self) -> None:
+        if self.cur_input > 0 and not self.parity_ready():
+            raise SBSError("LeftoverShards")
+        self.cur_input = 0
+
+    def reset_force(self) -> None:
+        self.cur_input = 0
+
+    def cur_input_index(self) -> int:
+        return self.cur_input
+
+    def encode(self, shards: Sequence) -> None:
+        if self.parity_ready():
+            raise SBSError("TooManyCalls")
+        try:
+            self.codec.encode_single(self.cur_input, shards)
+        except RsError as e:
+            raise SBSError("RSError", e) from None
+        self.cur_input += 1
+
+    def encode_sep(self, data: Sequence, parity: Sequence) -> None:
+        if self.parity_ready():
+            raise SBSError("TooManyCalls")
+        k, m = self.codec.data_shard_count(), self.codec.parity_shard_count()
+        # sbs_encode_sep_checks: data and parity piece counts, equal slices
+        try:
+            if len(data) != k:
+                raise RsError(3 if len(data) < k else 4)
+            if len(parity) != m:
+                raise RsError(5 if len(parity) < m else 6)
+            # check_slices!(multi => data, multi => parity), src/macros.rs:172-178
+            for group in (data, parity):
+                if len(group[0]) == 0:
+                    raise RsError(11)
+                if any(len(x) != len(group[0]) for x in group):
+                    raise RsError(9)
+            if len(data[0]) != len(parity[0]):
+                raise RsError(9)
+            self.codec.encode_single_sep(self.cur_input, data[self.cur_input], parity)
+        except RsError as e:
+            raise SBSError("RSError", e) from None
+        self.cur_input += 1

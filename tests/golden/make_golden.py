@@ -144,6 +144,16 @@ def main():
     p = t.index("assert_eq!(255, tables.log_lut[0]);")
     kats["lgf8_table_invariants"] = {"where": f"{rel}:{line_of(t, p)}", "log_lut0": 255, "exp_lut0": 1}
 
+    # --- encoding-format stable identity (tests/encoding_format_identity.rs)
+    rel = "tests/encoding_format_identity.rs"
+    t = read(rel)
+    for name, key in (("GF8_ID_V1", "format_id_gf8_custom_1x1"), ("TOWER_GF16_ID_V1", "format_id_tower_custom_1x1")):
+        p = t.index(f"const {name}: &[u8] =")
+        body, _ = bracket_after(t, t.index("=", p))
+        kats[key] = {"where": f"{rel}:{line_of(t, p)}", "bytes": parse_ints(body)}
+    kats["format_id_gf8_custom_1x1"]["custom_row"] = [0x87]
+    kats["format_id_tower_custom_1x1"]["custom_row"] = [[0x12, 0x34]]
+
     with open(OUT, "w") as f:
         json.dump(kats, f, indent=1, sort_keys=True)
     print("wrote", OUT)
