@@ -341,14 +341,24 @@ struct LeopardState {
   uint32_t m = 0, n = 0, mtrunc = 0, last = 0;
   std::mutex mu;
   std::unordered_map<std::string, LeoPlan> plans;
-  std::vector<void *> owned;
+  std::vector<void *> owned;    // retired scratch slabs, freed with the codec
+  // Locator arrays of the cached plans are carved from these slabs (plans
+  // live as long as the codec), so a new pattern costs no cudaMalloc.
+  std::vector<void *> plan_slabs;
+  size_t slab_used = 0, slab_bytes = 0;
   uint32_t *scratch = nullptr;  // global work rows for the decode of very wide codes
   size_t scratch_bytes = 0;
+  // Launches that use `scratch` are ordered across streams by this event:
+  // each waits for the previous user's record, then records its own.
+  cudaEvent_t scratch_done = nullptr;
+  std::mutex scratch_mu;
   std::vector<uint8_t> dense_enc;  // GF(2^8): the encode map as an m x k matrix
   ~LeopardState() {
     cudaDeviceSynchronize();
-    for (auto &kv : plans) cudaFree(kv.second.err);
+    for (void *p : plan_slabs) cudaFree(p);
     if (scratch) cudaFree(scratch);
+    for (void *p : owned) cudaFree(p);
+    if (scratch_done) cudaEventDestroy(scratch_done);
   }
 };
 
@@ -358,13 +368,35 @@ struct LeoLaunch {
   int engine = 1;  // 1: register-stage kernels, 0: half-warp layer kernels
   LeoArgs args{};
   void *d_blob = nullptr;  // jobs | pointers | roles
+  // One-shot launches allocate the blob on their stream and free it there
+  // after the kernel; prepared launches own it until destroyed.
+  bool blob_ordered = false;
+  cudaStream_t blob_stream = nullptr;
   int grid = 0;
   size_t smem = 0;
   bool global_work = false;
   ~LeoLaunch() {
-    if (d_blob) cudaFree(d_blob);
+    if (!d_blob) return;
+    if (blob_ordered)
+      cudaFreeAsync(d_blob, blob_stream);
+    else
+      cudaFree(d_blob);
   }
 };
+
+// Grow the codec's scratch slab to `need` bytes.  A slab another thread may
+// still have in a built launch is retired (kept until the codec is
+// destroyed), never freed under it.
+int grow_scratch(LeopardState &st, size_t need) {
+  std::lock_guard<std::mutex> g(st.scratch_mu);
+  if (st.scratch_bytes >= need) return RSGPU_OK;
+  if (st.scratch) st.owned.push_back(st.scratch);
+  st.scratch = nullptr;
+  st.scratch_bytes = 0;
+  RS_CUDA(cudaMalloc(&st.scratch, need));
+  st.scratch_bytes = need;
+  return RSGPU_OK;
+}
 
 int Codec::init_leopard() {
   RS_CUDA(cudaGetDevice(&device));
@@ -517,17 +549,12 @@ int configure_fft(const K kernel, LeoLaunch &L, uint32_t rows, uint32_t reg_lane
     L.smem = 0;
     L.grid = int(std::min<uint64_t>(tiles, uint64_t(2 * sm_count())));
     const size_t need = size_t(L.grid) * rows * nb * 64;
-    if (st.scratch_bytes < need) {
-      if (st.scratch) {
-        RS_CUDA(cudaDeviceSynchronize());
-        cudaFree(st.scratch);
-        st.scratch = nullptr;
-        st.scratch_bytes = 0;
-      }
-      RS_CUDA(cudaMalloc(&st.scratch, need));
-      st.scratch_bytes = need;
+    int rc = grow_scratch(st, need);
+    if (rc) return rc;
+    {
+      std::lock_guard<std::mutex> g(st.scratch_mu);
+      L.args.scratch = st.scratch;
     }
-    L.args.scratch = st.scratch;
   }
   return RSGPU_OK;
 }
@@ -551,17 +578,12 @@ int configure(const K kernel, LeoLaunch &L, uint32_t lanes, size_t len, uint64_t
     L.smem = 0;
     L.grid = int(std::min<uint64_t>(tiles, uint64_t(2 * sm_count())));
     const size_t need = size_t(L.grid) * lanes * nb * 64;
-    if (st.scratch_bytes < need) {
-      if (st.scratch) {
-        RS_CUDA(cudaDeviceSynchronize());
-        cudaFree(st.scratch);
-        st.scratch = nullptr;
-        st.scratch_bytes = 0;
-      }
-      RS_CUDA(cudaMalloc(&st.scratch, need));
-      st.scratch_bytes = need;
+    int rc = grow_scratch(st, need);
+    if (rc) return rc;
+    {
+      std::lock_guard<std::mutex> g(st.scratch_mu);
+      L.args.scratch = st.scratch;
     }
-    L.args.scratch = st.scratch;
   }
   return RSGPU_OK;
 }
@@ -578,7 +600,17 @@ int decode_plan(Codec &c, const uint8_t *present, LeoPlan **out, cudaStream_t s,
     return RSGPU_OK;
   }
   LeoPlan plan;
-  RS_CUDA(cudaMalloc(&plan.err, st.n * 2));
+  const size_t bytes = (size_t(st.n) * 2 + 255) & ~size_t(255);
+  if (st.plan_slabs.empty() || st.slab_used + bytes > st.slab_bytes) {
+    const size_t sz = std::max<size_t>(size_t(1) << 20, bytes);
+    void *p = nullptr;
+    RS_CUDA(cudaMalloc(&p, sz));
+    st.plan_slabs.push_back(p);
+    st.slab_used = 0;
+    st.slab_bytes = sz;
+  }
+  plan.err = reinterpret_cast<uint16_t *>(static_cast<uint8_t *>(st.plan_slabs.back()) + st.slab_used);
+  st.slab_used += bytes;
   plan.input_count = st.m;
   for (size_t i = 0; i < c.k; ++i)
     if (present[i]) plan.input_count = uint32_t(st.m + i + 1);
@@ -595,9 +627,10 @@ int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>
   const size_t total = c.k + c.m;
   std::vector<uint8_t> pres(pending.size() * total);
   for (size_t i = 0; i < pending.size(); ++i) std::memcpy(&pres[i * total], pending[i].first.data(), total);
+  // Stream-ordered scratch: nothing here waits for other streams' work.
   uint8_t *d_pres = nullptr;
-  RS_CUDA(cudaMalloc(&d_pres, pres.size()));
-  RS_CUDA(cudaMemcpy(d_pres, pres.data(), pres.size(), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&d_pres), pres.size(), s));
+  RS_CUDA(cudaMemcpyAsync(d_pres, pres.data(), pres.size(), cudaMemcpyHostToDevice, s));
   std::vector<const uint8_t *> pp(pending.size());
   std::vector<uint16_t *> oo(pending.size());
   for (size_t i = 0; i < pending.size(); ++i) {
@@ -605,10 +638,10 @@ int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>
     oo[i] = st.plans[pending[i].first].err;
   }
   void *d_pp = nullptr, *d_oo = nullptr;
-  RS_CUDA(cudaMalloc(&d_pp, pp.size() * sizeof(void *)));
-  RS_CUDA(cudaMalloc(&d_oo, oo.size() * sizeof(void *)));
-  RS_CUDA(cudaMemcpy(d_pp, pp.data(), pp.size() * sizeof(void *), cudaMemcpyHostToDevice));
-  RS_CUDA(cudaMemcpy(d_oo, oo.data(), oo.size() * sizeof(void *), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMallocAsync(&d_pp, pp.size() * sizeof(void *), s));
+  RS_CUDA(cudaMallocAsync(&d_oo, oo.size() * sizeof(void *), s));
+  RS_CUDA(cudaMemcpyAsync(d_pp, pp.data(), pp.size() * sizeof(void *), cudaMemcpyHostToDevice, s));
+  RS_CUDA(cudaMemcpyAsync(d_oo, oo.data(), oo.size() * sizeof(void *), cudaMemcpyHostToDevice, s));
   const int bits = st.field->bits;
   const size_t smem = size_t(1u << bits) * 2;
   if (bits == 16) {
@@ -623,17 +656,19 @@ int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>
   }
   launch_counter_add(1);
   RS_CUDA(cudaGetLastError());
+  cudaFreeAsync(d_pres, s);
+  cudaFreeAsync(d_pp, s);
+  cudaFreeAsync(d_oo, s);
+  // The new plans are visible to other streams once the lock is released,
+  // so their locators must be complete: wait for this stream only.
   RS_CUDA(cudaStreamSynchronize(s));
-  cudaFree(d_pres);
-  cudaFree(d_pp);
-  cudaFree(d_oo);
   pending.clear();
   return RSGPU_OK;
 }
 
 int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
               int goal, const uint8_t *required, size_t n_required, uint32_t *flags, LeoLaunch &L,
-              cudaStream_t s) {
+              cudaStream_t s, bool one_shot) {
   LeopardState &st = *c.leo;
   const size_t total = c.k + c.m;
   L.codec = &c;
@@ -687,12 +722,21 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
   std::vector<uint8_t> blob(jb + pb + roles.size() + 16);
   std::memcpy(blob.data() + jb, shards, pb);
   std::memcpy(blob.data() + jb + pb, roles.data(), roles.size());
-  RS_CUDA(cudaMalloc(&L.d_blob, std::max<size_t>(blob.size(), 16)));
+  if (one_shot) {
+    RS_CUDA(cudaMallocAsync(&L.d_blob, std::max<size_t>(blob.size(), 16), s));
+    L.blob_ordered = true;
+    L.blob_stream = s;
+  } else {
+    RS_CUDA(cudaMalloc(&L.d_blob, std::max<size_t>(blob.size(), 16)));
+  }
   uint8_t *dbase = static_cast<uint8_t *>(L.d_blob);
   for (size_t i = 0; i < jobs.size(); ++i)
     if (L.decode) jobs[i].role = dbase + jb + pb + role_off[i];
   std::memcpy(blob.data(), jobs.data(), jb);
-  RS_CUDA(cudaMemcpy(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  if (one_shot)
+    RS_CUDA(cudaMemcpyAsync(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, s));
+  else
+    RS_CUDA(cudaMemcpy(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
   LeoArgs &a = L.args;
   a.jobs = reinterpret_cast<const LeoJob *>(dbase);
   a.ptrs = reinterpret_cast<const uint8_t *const *>(dbase + jb);
@@ -743,8 +787,31 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
 
 }  // namespace
 
+namespace {
+int leo_launch_kernel(const LeoLaunch &L, cudaStream_t s);
+}
+
+// Launches that use the codec's shared scratch slab (global work rows) wait
+// for the previous such launch on any stream.  Under stream capture the
+// graph's own dependencies order them instead (an event recorded outside a
+// capture cannot be waited on inside it).
 int leo_launch(const LeoLaunch &L, cudaStream_t s) {
   if (L.args.n_jobs == 0) return RSGPU_OK;
+  if (!L.global_work) return leo_launch_kernel(L, s);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  RS_CUDA(cudaStreamIsCapturing(s, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return leo_launch_kernel(L, s);
+  LeopardState &st = *L.codec->leo;
+  std::lock_guard<std::mutex> g(st.scratch_mu);
+  if (!st.scratch_done) RS_CUDA(cudaEventCreateWithFlags(&st.scratch_done, cudaEventDisableTiming));
+  RS_CUDA(cudaStreamWaitEvent(s, st.scratch_done, 0));
+  int rc = leo_launch_kernel(L, s);
+  if (rc) return rc;
+  return cuda_status(cudaEventRecord(st.scratch_done, s));
+}
+
+namespace {
+int leo_launch_kernel(const LeoLaunch &L, cudaStream_t s) {
   const bool b16 = L.codec->leo->field->bits == 16;
   const LeoArgs &a = L.args;
   if (L.engine == 1) {
@@ -798,6 +865,7 @@ int leo_launch(const LeoLaunch &L, cudaStream_t s) {
   launch_counter_add(1);
   return cuda_status(cudaGetLastError());
 }
+}  // namespace
 
 uint32_t leo_kernel_count(const LeoLaunch &L) { return L.args.n_jobs ? 1 : 0; }
 
@@ -805,7 +873,7 @@ int prepare_other(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, co
                   int goal, uint32_t *flags, std::shared_ptr<LeoLaunch> &out) {
   if (c.family == RSGPU_FAMILY_CLASSIC) return prepare_tower(c, op, n_stripes, shards, present, len, goal, flags, out);
   auto L = std::make_shared<LeoLaunch>();
-  int rc = build_leo(c, op, n_stripes, shards, present, len, goal, nullptr, 0, flags, *L, nullptr);
+  int rc = build_leo(c, op, n_stripes, shards, present, len, goal, nullptr, 0, flags, *L, nullptr, false);
   if (rc) return rc;
   out = L;
   return RSGPU_OK;
@@ -813,14 +881,12 @@ int prepare_other(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, co
 
 static int run_once(Codec &c, int op, size_t n, uint8_t *const *shards, const uint8_t *present, size_t len, int goal,
                     const uint8_t *required, size_t n_required, uint32_t *flags, cudaStream_t s) {
+  // Stream-ordered: the launch's job blob is freed on `s` behind the kernel
+  // when L goes out of scope, so the call returns without waiting.
   LeoLaunch L;
-  int rc = build_leo(c, op, n, shards, present, len, goal, required, n_required, flags, L, s);
+  int rc = build_leo(c, op, n, shards, present, len, goal, required, n_required, flags, L, s, true);
   if (rc) return rc;
-  rc = leo_launch(L, s);
-  if (rc) return rc;
-  // The launch's tables are freed with L; wait for the kernel first.
-  RS_CUDA(cudaStreamSynchronize(s));
-  return RSGPU_OK;
+  return leo_launch(L, s);
 }
 
 int leopard_encode(Codec &c, size_t n, uint8_t *const *shards, size_t len, cudaStream_t s) {
@@ -829,15 +895,15 @@ int leopard_encode(Codec &c, size_t n, uint8_t *const *shards, size_t len, cudaS
 
 int leopard_verify(Codec &c, size_t n, const uint8_t *const *shards, size_t len, uint8_t *ok, cudaStream_t s) {
   uint32_t *flags = nullptr;
-  RS_CUDA(cudaMalloc(&flags, std::max<size_t>(n, 1) * 4));
+  RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&flags), std::max<size_t>(n, 1) * 4, s));
   RS_CUDA(cudaMemsetAsync(flags, 0, std::max<size_t>(n, 1) * 4, s));
   int rc = run_once(c, RSGPU_OP_VERIFY, n, const_cast<uint8_t *const *>(shards), nullptr, len, 0, nullptr, 0, flags, s);
   std::vector<uint32_t> f(n);
-  if (rc == RSGPU_OK) {
-    RS_CUDA(cudaMemcpy(f.data(), flags, n * 4, cudaMemcpyDeviceToHost));
+  if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpyAsync(f.data(), flags, n * 4, cudaMemcpyDeviceToHost, s));
+  cudaFreeAsync(flags, s);
+  if (rc == RSGPU_OK) rc = cuda_status(cudaStreamSynchronize(s));
+  if (rc == RSGPU_OK)
     for (size_t i = 0; i < n; ++i) ok[i] = f[i] ? 0 : 1;
-  }
-  cudaFree(flags);
   return rc;
 }
 
@@ -940,14 +1006,18 @@ int leopard_dense_encode(Codec &c, std::vector<uint8_t> &rows) {
   std::vector<uint8_t> host(total * L, 0);
   const uint8_t one = leo8_one();
   for (size_t j = 0; j < k; ++j) host[j * L + j] = one;
+  cudaStream_t s = nullptr;
+  RS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   uint8_t *d = nullptr;
-  RS_CUDA(cudaMalloc(&d, host.size()));
-  RS_CUDA(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
+  int rc = cuda_status(cudaMallocAsync(reinterpret_cast<void **>(&d), host.size(), s));
+  if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, s));
   std::vector<uint8_t *> ptrs(total);
   for (size_t i = 0; i < total; ++i) ptrs[i] = d + i * L;
-  int rc = leopard_encode(c, 1, ptrs.data(), L, nullptr);
-  if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpy(host.data(), d, host.size(), cudaMemcpyDeviceToHost));
-  cudaFree(d);
+  if (rc == RSGPU_OK) rc = leopard_encode(c, 1, ptrs.data(), L, s);
+  if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpyAsync(host.data(), d, host.size(), cudaMemcpyDeviceToHost, s));
+  if (d) cudaFreeAsync(d, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess && rc == RSGPU_OK) rc = RSGPU_ERR_CUDA;
+  cudaStreamDestroy(s);
   if (rc) return rc;
   rows.assign(m * k, 0);
   for (size_t r = 0; r < m; ++r)
@@ -983,14 +1053,16 @@ int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, s
   const uint8_t one = leo8_one();
   for (size_t i = 0; i < n; ++i)
     for (size_t q = 0; q < maps[i].inputs.size(); ++q) host[(i * total + maps[i].inputs[q]) * L + q] = one;
+  // Stream-ordered on `s`; the host waits for `s` only, to read the maps.
   uint8_t *d = nullptr;
-  RS_CUDA(cudaMalloc(&d, host.size()));
-  RS_CUDA(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&d), host.size(), s));
+  int rc = cuda_status(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, s));
   std::vector<uint8_t *> ptrs(n * total);
   for (size_t i = 0; i < n * total; ++i) ptrs[i] = d + i * L;
-  int rc = leopard_reconstruct(c, n, ptrs.data(), present, L, goal, nullptr, 0, s);
-  if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpy(host.data(), d, host.size(), cudaMemcpyDeviceToHost));
-  cudaFree(d);
+  if (rc == RSGPU_OK) rc = leopard_reconstruct(c, n, ptrs.data(), present, L, goal, nullptr, 0, s);
+  if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpyAsync(host.data(), d, host.size(), cudaMemcpyDeviceToHost, s));
+  cudaFreeAsync(d, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess && rc == RSGPU_OK) rc = RSGPU_ERR_CUDA;
   if (rc) return rc;
   for (size_t i = 0; i < n; ++i) {
     LeoDenseMap &mp = maps[i];
