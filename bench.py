@@ -466,19 +466,23 @@ def main():
     # End to end through the public API with pinned host buffers.
     e2e = e2e_measure(torch, rsgpu, args, rank)
 
+    for item in work:
+        item.clear()  # drops the config-2 shard buffers (137 GiB)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    # Config 1 (the reference's CPU-runnable case) and config 3 (Leopard
+    # GF(2^16) 1024+512): per-operation times, bytes checked.
+    config1 = config1_workload(torch, rsgpu, stream, gen)
+    leopard16 = leopard16_workload(torch, rsgpu, stream, gen)
+    torch.cuda.empty_cache()
+
     # Mixed geometries in one persistent kernel (batched, model-scheduled)
     # against the per-stripe kernel loop.
     mixed = None
     if not args.no_mix:
-        for item in work:
-            item.clear()  # drops the config-2 shard buffers (137 GiB)
-        torch.cuda.synchronize()
-        torch.cuda.empty_cache()
         mixed = mixed_workload(args, torch, rsgpu, rank, stream, gen)
     serving = None
     if not args.no_serve:
-        for item in work:
-            item.clear()
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
         serving = serving_workload(args, torch, rsgpu, rank, gen)
@@ -509,6 +513,8 @@ def main():
                            "batched_same_stripes": round(batched_same, 1),
                            "batched_speedup": round(batched_same / ps_value, 3)},
             "clocks": clk.summary(),
+            "config1": config1,
+            "leopard_gf16": leopard16,
             "mixed": mixed,
             "serving": serving,
             "e2e": e2e,
@@ -520,6 +526,92 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _median_ms(torch, stream, fn, reps):
+    """Median CUDA-event time of fn() on `stream` over reps launches."""
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts)), float(np.percentile(ts, 99))
+
+
+def config1_workload(torch, rsgpu, stream, gen):
+    """Classic 10+4, 64 KiB shards, 256 stripes: encode, erase {0,3,11,13},
+    reconstruct, verify; every byte checked against the original stripes.
+    Times are per operation over all 256 stripes (inputs 235 MB > L2)."""
+    k, m, size, n = 10, 4, 65536, 256
+    codec = rsgpu.ReedSolomon(k, m)
+    buf = torch.empty((n, k + m, size), dtype=torch.uint8, device="cuda")
+    buf[:, :k].random_(0, 256, generator=gen)
+    offs = np.arange(n * (k + m), dtype=np.uint64) * np.uint64(size)
+    ptrs = rsgpu.device_pointer_table(buf.data_ptr(), offs)
+    enc = codec.prepare_batch("encode", ptrs, size)
+    enc.launch()
+    torch.cuda.synchronize()
+    orig = buf.clone()
+    pats = np.ones((n, k + m), np.uint8)
+    pats[:, [0, 3, 11, 13]] = 0
+    buf[:, [0, 3, 11, 13]] = 0
+    rec = codec.prepare_batch("reconstruct", ptrs, size, present=pats)
+    ver = codec.prepare_batch("verify", ptrs, size)
+    rec.launch()
+    ver.launch()
+    torch.cuda.synchronize()
+    exact = bool(torch.equal(buf, orig)) and bool(ver.verify_result().all())
+    out = {"workload": "classic 10+4, 64 KiB shards, 256 stripes, erase {0,3,11,13}", "bit_exact": exact}
+    nbytes = n * (k + m) * size  # encode, reconstruct ((k + 4) S) and verify move the same bytes
+    for name, b in (("encode", enc), ("reconstruct", rec), ("verify", ver)):
+        med, p99 = _median_ms(torch, stream, b.launch, 20)
+        out[name] = {"us": round(med * 1e3, 1), "p99_us": round(p99 * 1e3, 1),
+                     "gbs": round(nbytes / (med / 1e3) / 1e9, 1)}
+    del buf, orig
+    return out
+
+
+def leopard16_workload(torch, rsgpu, stream, gen):
+    """Leopard GF(2^16) k=1024, m=512, 16 KiB shards, 64 stripes (1.6 GB):
+    encode, erase 512 seeded shards per stripe, reconstruct; the rebuilt
+    stripes must equal the originals byte for byte.  Multiply-XOR counts per
+    element column: encode 2 * 256 * 9 (two IFFT chunks of 512) + 256 * 9
+    (the FFT), decode 2 * 1024 * 11 (IFFT and FFT of n = 2048)."""
+    k, m, size, n = 1024, 512, 16384, 64
+    codec = rsgpu.ReedSolomon(k, m, rsgpu.CodecOptions(codec_family="leopard_gf16"))
+    buf = torch.empty((n, k + m, size), dtype=torch.uint8, device="cuda")
+    buf[:, :k].random_(0, 256, generator=gen)
+    offs = np.arange(n * (k + m), dtype=np.uint64) * np.uint64(size)
+    ptrs = rsgpu.device_pointer_table(buf.data_ptr(), offs)
+    enc = codec.prepare_batch("encode", ptrs, size)
+    enc.launch()
+    torch.cuda.synchronize()
+    orig = buf.clone()
+    rng = np.random.default_rng(SEED + 3)
+    pats = np.ones((n, k + m), np.uint8)
+    for s in range(n):
+        pats[s, rng.choice(k + m, size=m, replace=False)] = 0
+    lost = torch.from_numpy(pats == 0).cuda()
+    buf.masked_fill_(lost.unsqueeze(-1), 0)
+    rec = codec.prepare_batch("reconstruct", ptrs, size, present=pats)
+    rec.launch()
+    torch.cuda.synchronize()
+    exact = bool(torch.equal(buf, orig))
+    cols = size // 2
+    mx = {"encode": (2 * 256 * 9 + 256 * 9) * cols * n, "reconstruct": 2 * 1024 * 11 * cols * n}
+    nbytes = n * (k + m) * size  # encode reads k, writes m; reconstruct reads k + m - e, writes e
+    out = {"workload": "Leopard GF16 1024+512, 16 KiB shards, 64 stripes, 512 seeded erasures each",
+           "bit_exact": exact}
+    for name, b in (("encode", enc), ("reconstruct", rec)):
+        med, p99 = _median_ms(torch, stream, b.launch, 10)
+        out[name] = {"ms": round(med, 3), "p99_ms": round(p99, 3),
+                     "gbs": round(nbytes / (med / 1e3) / 1e9, 1),
+                     "mul_xor_per_s": float(f"{mx[name] / (med / 1e3):.4g}")}
+    del buf, orig
+    return out
 
 
 def mixed_workload(args, torch, rsgpu, rank, stream, gen):
