@@ -228,8 +228,10 @@ __host__ __device__ inline uint64_t fft_tile_bytes(uint32_t lanes_one_thread, ui
   return lanes_one_thread <= 16 ? uint64_t(4 * kFftThreads) : uint64_t(64) * nb;
 }
 
-template <int BITS, bool VERIFY, bool GLOBAL_WORK>
-__global__ void __launch_bounds__(kFftThreads, 2) k_fft_encode(LeoArgs a) {
+// NT = 512 is used when a tile's shared memory leaves room for one CTA per
+// SM: 16 warps instead of 8 on the same rows, at the same 128-register cap.
+template <int BITS, bool VERIFY, bool GLOBAL_WORK, int NT = kFftThreads>
+__global__ void __launch_bounds__(NT, NT == kFftThreads ? 2 : 1) k_fft_encode(LeoArgs a) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint32_t bad;
   uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
@@ -240,12 +242,12 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_fft_encode(LeoArgs a) {
     const uint32_t job = t / tiles_per_job;
     const uint64_t col0 = uint64_t(t - job * tiles_per_job) * tile_bytes;
     const LeoJob jd = a.jobs[job];
-    fft_encode_tile<BITS, VERIFY, kFftThreads>(W, a, jd, col0, a.len, &bad);
+    fft_encode_tile<BITS, VERIFY, NT>(W, a, jd, col0, a.len, &bad);
   }
 }
 
-template <int BITS, bool GLOBAL_WORK>
-__global__ void __launch_bounds__(kFftThreads, 2) k_fft_decode(LeoArgs a) {
+template <int BITS, bool GLOBAL_WORK, int NT = kFftThreads>
+__global__ void __launch_bounds__(NT, NT == kFftThreads ? 2 : 1) k_fft_decode(LeoArgs a) {
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
   const uint64_t tile_bytes = fft_tile_bytes(a.n, a.nb);
@@ -255,7 +257,7 @@ __global__ void __launch_bounds__(kFftThreads, 2) k_fft_decode(LeoArgs a) {
     const uint32_t job = t / tiles_per_job;
     const uint64_t col0 = uint64_t(t - job * tiles_per_job) * tile_bytes;
     const LeoJob jd = a.jobs[job];
-    fft_decode_tile<BITS, kFftThreads>(W, a, jd, col0, a.len);
+    fft_decode_tile<BITS, NT>(W, a, jd, col0, a.len);
   }
 }
 
@@ -372,6 +374,7 @@ struct LeoLaunch {
   // after the kernel; prepared launches own it until destroyed.
   bool blob_ordered = false;
   cudaStream_t blob_stream = nullptr;
+  int threads = 256;  // register-stage kernels: 256, or 512 for one CTA per SM
   int grid = 0;
   size_t smem = 0;
   bool global_work = false;
@@ -525,8 +528,9 @@ constexpr size_t kFftSmemBudget = 96 * 1024;  // two resident CTAs per SM
 // Work rows and tile width of a register-stage launch: `rows` rows of work
 // (encoder 2m, decoder n) when the transform needs shared memory, i.e. when
 // `reg_lanes` (m or n) exceeds 16.
-template <class K>
-int configure_fft(const K kernel, LeoLaunch &L, uint32_t rows, uint32_t reg_lanes, size_t len, size_t n_jobs) {
+template <class K, class K2>
+int configure_fft(const K kernel, const K2 kernel_wide, LeoLaunch &L, uint32_t rows, uint32_t reg_lanes, size_t len,
+                  size_t n_jobs) {
   LeopardState &st = *L.codec->leo;
   L.args.lanes = rows;
   size_t smem = 0;
@@ -539,15 +543,24 @@ int configure_fft(const K kernel, LeoLaunch &L, uint32_t rows, uint32_t reg_lane
   L.global_work = smem > 200 * 1024;
   const uint64_t tile = fft_tile_bytes(reg_lanes, nb);
   const uint64_t tiles = ((len + tile - 1) / tile) * std::max<size_t>(n_jobs, 1);
+  L.threads = kFftThreads;
   if (!L.global_work) {
     L.smem = smem;
-    if (smem > 48 * 1024) RS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    const void *fn = reinterpret_cast<const void *>(kernel);
+    if (smem > kFftSmemBudget) {  // one CTA per SM: give it twice the warps
+      L.threads = 2 * kFftThreads;
+      fn = reinterpret_cast<const void *>(kernel_wide);
+    }
+    if (smem > 48 * 1024) RS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
-    RS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFftThreads, smem));
+    RS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, L.threads, smem));
     L.grid = int(std::min<uint64_t>(tiles, uint64_t(std::max(per_sm, 1)) * sm_count()));
   } else {
+    // Work rows in a global slab (L2-resident): one 512-thread CTA per SM
+    // keeps the slab half the size of two 256-thread CTAs per SM.
     L.smem = 0;
-    L.grid = int(std::min<uint64_t>(tiles, uint64_t(2 * sm_count())));
+    L.threads = 2 * kFftThreads;
+    L.grid = int(std::min<uint64_t>(tiles, uint64_t(sm_count())));
     const size_t need = size_t(L.grid) * rows * nb * 64;
     int rc = grow_scratch(st, need);
     if (rc) return rc;
@@ -759,13 +772,17 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
     const bool b16f = st.field->bits == 16;
     const size_t nj = jobs.size();
     if (L.decode)
-      return b16f ? configure_fft(k_fft_decode<16, false>, L, st.n, st.n, len, nj)
-                  : configure_fft(k_fft_decode<8, false>, L, st.n, st.n, len, nj);
+      return b16f ? configure_fft(k_fft_decode<16, false>, k_fft_decode<16, false, 512>, L, st.n, st.n, len, nj)
+                  : configure_fft(k_fft_decode<8, false>, k_fft_decode<8, false, 512>, L, st.n, st.n, len, nj);
     if (L.verify)
-      return b16f ? configure_fft(k_fft_encode<16, true, false>, L, 2 * st.m, st.m, len, nj)
-                  : configure_fft(k_fft_encode<8, true, false>, L, 2 * st.m, st.m, len, nj);
-    return b16f ? configure_fft(k_fft_encode<16, false, false>, L, 2 * st.m, st.m, len, nj)
-                : configure_fft(k_fft_encode<8, false, false>, L, 2 * st.m, st.m, len, nj);
+      return b16f ? configure_fft(k_fft_encode<16, true, false>, k_fft_encode<16, true, false, 512>, L, 2 * st.m,
+                                  st.m, len, nj)
+                  : configure_fft(k_fft_encode<8, true, false>, k_fft_encode<8, true, false, 512>, L, 2 * st.m, st.m,
+                                  len, nj);
+    return b16f ? configure_fft(k_fft_encode<16, false, false>, k_fft_encode<16, false, false, 512>, L, 2 * st.m,
+                                st.m, len, nj)
+                : configure_fft(k_fft_encode<8, false, false>, k_fft_encode<8, false, false, 512>, L, 2 * st.m, st.m,
+                                len, nj);
   }
   const uint32_t lanes = L.decode ? st.n : 2 * st.m;
   const uint32_t nb_guess = pick_nb(lanes, len);
@@ -815,23 +832,30 @@ int leo_launch_kernel(const LeoLaunch &L, cudaStream_t s) {
   const bool b16 = L.codec->leo->field->bits == 16;
   const LeoArgs &a = L.args;
   if (L.engine == 1) {
-    const dim3 grid(L.grid), block(kFftThreads);
+    const dim3 grid(L.grid), block(L.threads);
+    const bool wide = L.threads != kFftThreads;
 #define FFT_GO(KERNEL) KERNEL<<<grid, block, L.smem, s>>>(a)
     if (L.decode) {
       if (L.global_work) {
-        if (b16) FFT_GO((k_fft_decode<16, true>)); else FFT_GO((k_fft_decode<8, true>));
+        if (b16) FFT_GO((k_fft_decode<16, true, 512>)); else FFT_GO((k_fft_decode<8, true, 512>));
+      } else if (wide) {
+        if (b16) FFT_GO((k_fft_decode<16, false, 512>)); else FFT_GO((k_fft_decode<8, false, 512>));
       } else {
         if (b16) FFT_GO((k_fft_decode<16, false>)); else FFT_GO((k_fft_decode<8, false>));
       }
     } else if (L.verify) {
       if (L.global_work) {
-        if (b16) FFT_GO((k_fft_encode<16, true, true>)); else FFT_GO((k_fft_encode<8, true, true>));
+        if (b16) FFT_GO((k_fft_encode<16, true, true, 512>)); else FFT_GO((k_fft_encode<8, true, true, 512>));
+      } else if (wide) {
+        if (b16) FFT_GO((k_fft_encode<16, true, false, 512>)); else FFT_GO((k_fft_encode<8, true, false, 512>));
       } else {
         if (b16) FFT_GO((k_fft_encode<16, true, false>)); else FFT_GO((k_fft_encode<8, true, false>));
       }
     } else {
       if (L.global_work) {
-        if (b16) FFT_GO((k_fft_encode<16, false, true>)); else FFT_GO((k_fft_encode<8, false, true>));
+        if (b16) FFT_GO((k_fft_encode<16, false, true, 512>)); else FFT_GO((k_fft_encode<8, false, true, 512>));
+      } else if (wide) {
+        if (b16) FFT_GO((k_fft_encode<16, false, false, 512>)); else FFT_GO((k_fft_encode<8, false, false, 512>));
       } else {
         if (b16) FFT_GO((k_fft_encode<16, false, false>)); else FFT_GO((k_fft_encode<8, false, false>));
       }

@@ -162,6 +162,35 @@ def test_lgf16_wide_code_uses_global_work(rs, torch):
         assert np.array_equal(lst[i].cpu().numpy(), full[i]), i
 
 
+@pytest.mark.parametrize("k,m,size", [(1024, 512, 256), (2048, 1024, 128), (4000, 1000, 64)])
+@pytest.mark.parametrize("codeword", [True, False])
+def test_lgf16_wide_decode_matches_oracle(rs, torch, k, m, size, codeword):
+    # 2048, 4096 and 8192 transform lanes: the decode's work rows exceed
+    # shared memory and live in a global slab.  Arbitrary (non-codeword)
+    # inputs pin the whole pipeline, not only the round trip.
+    rng = np.random.default_rng(k + m + size + int(codeword))
+    data = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)]
+    if codeword:
+        rc, par = O.leopard_encode(16, k, m, data)
+        assert rc == 0
+        full = data + par
+    else:
+        full = data + [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(m)]
+    c = codec(rs, 16, k, m)
+    for e in (m, int(rng.integers(1, m))):
+        lost = set(rng.choice(k + m, size=e, replace=False).tolist())
+        pres = [0 if i in lost else 1 for i in range(k + m)]
+        ref = [s.copy() for s in full]
+        for i in lost:
+            ref[i][:] = 0
+        assert O.leopard_reconstruct(16, k, m, ref, pres) == 0
+        buf = torch.from_numpy(np.stack(full)).cuda()
+        lst = [None if i in lost else buf[i] for i in range(k + m)]
+        c.reconstruct(lst)
+        for i in sorted(lost):
+            assert np.array_equal(lst[i].cpu().numpy(), ref[i]), (k, m, e, i)
+
+
 def test_leopard_errors(rs, torch):
     c = codec(rs, 8, 4, 2)
     sh = [torch.zeros(100, dtype=torch.uint8, device="cuda") for _ in range(6)]
