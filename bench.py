@@ -310,28 +310,22 @@ def main():
     if args.case:
         return PROFILE_CASES[args.case]()
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        return run_reference(args, rank, world)
+    if args.impl == "reference":  # the reference arm loads nothing of this package
+        return run_reference(args, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")))
 
     import torch
 
     import rsgpu
+    from rsgpu import ranks as R
 
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
+    rk = R.from_env()
+    rank, world = rk.rank, rk.world
 
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(rk.local)
+    group = R.Group(rk, "nccl", timeout_s=120.0, device="cuda")
 
     def barrier():
-        if dist:
-            dist.barrier()
+        group.barrier()
         torch.cuda.synchronize()
 
     stream = torch.cuda.current_stream()
@@ -389,10 +383,7 @@ def main():
         assert w["ver"].verify_result().all()
     gpu_launches = kern_per_step * args.steps
     assert rsgpu.kernel_launch_count() - launches0 == gpu_launches
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = group.max(ms)
     value = total_bytes * world / (ms_max / 1e3) / 1e9
 
     # Dominant kernel (10+4 encode) timed alone with events on its stream.
@@ -464,7 +455,7 @@ def main():
     del per, sub_batches
 
     # End to end through the public API with pinned host buffers.
-    e2e = e2e_measure(torch, rsgpu, args, rank)
+    e2e = e2e_measure(torch, rsgpu, args, group)
 
     for item in work:
         item.clear()  # drops the config-2 shard buffers (137 GiB)
@@ -522,9 +513,7 @@ def main():
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    group.close()
     return 0
 
 
@@ -834,10 +823,12 @@ def serving_workload(args, torch, rsgpu, rank, gen):
     return out
 
 
-def e2e_measure(torch, rsgpu, args, rank):
+def e2e_measure(torch, rsgpu, args, group):
     """Same operations through ReedSolomon.*_batch with pinned host shards: each
     step copies inputs host->device and results (parity, rebuilt shards, verify
-    flags) device->host inside the timed region."""
+    flags) device->host inside the timed region.  Every rank runs the same
+    per-GPU work; the figure is all ranks' bytes over the slowest rank's
+    time."""
     n = args.e2e_stripes
     stripes = []
     h2d = d2h = 0
@@ -869,11 +860,15 @@ def e2e_measure(torch, rsgpu, args, rank):
     step()
     steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize()
+    group.barrier()
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
     torch.cuda.synchronize()
-    dt = (time.perf_counter() - t0) / steps
+    dt = group.max((time.perf_counter() - t0) / steps)
+    total *= group.ranks.world
+    h2d *= group.ranks.world
+    d2h *= group.ranks.world
     for codec, lists, pats, host in stripes:
         del host
     return {"value": round(total / dt / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
