@@ -371,7 +371,7 @@ def main():
     launches0 = rsgpu.kernel_launch_count()
     kern_per_step = sum(w[x].kernel_count() for w in work for x in ("enc", "rec", "ver"))
     st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    with ClockSampler(rk.local) as clk:
         barrier()
         st.record(stream)
         for _ in range(args.steps):
