@@ -866,13 +866,41 @@ def e2e_measure(torch, rsgpu, args, group):
         step()
     torch.cuda.synchronize()
     dt = group.max((time.perf_counter() - t0) / steps)
+    for codec, lists, pats, host in stripes:
+        del host
+    link = host_link_gbs(torch)
+    # The link's own bound for this step: the two directions use separate copy
+    # engines, so the larger of the two transfer times.
+    bound = max(h2d / (link["h2d_gbs"] * 1e9), d2h / (link["d2h_gbs"] * 1e9))
     total *= group.ranks.world
     h2d *= group.ranks.world
     d2h *= group.ranks.world
-    for codec, lists, pats, host in stripes:
-        del host
     return {"value": round(total / dt / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "stripes_per_geometry": n, "api": "ReedSolomon.*_batch, host memory"}
+            "d2h_bytes_per_step": int(d2h), "stripes_per_geometry": n, "api": "ReedSolomon.*_batch, host memory",
+            "s_per_step": round(dt, 4), "link": link, "link_bound_s_per_step": round(bound, 4),
+            "link_frac": round(bound / dt, 3)}
+
+
+def host_link_gbs(torch, nbytes=2 << 30, reps=5):
+    """Pinned host <-> device copy bandwidth of this GPU (one 2 GiB copy each
+    way, best of reps, CUDA events): the ceiling of the host-memory path."""
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    out = {}
+    for name, fn in (("h2d_gbs", lambda: d.copy_(h, non_blocking=True)),
+                     ("d2h_gbs", lambda: h.copy_(d, non_blocking=True))):
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            best = t if best is None else min(best, t)
+        out[name] = round(nbytes / best / 1e9, 1)
+    del h, d
+    return out
 
 
 if __name__ == "__main__":

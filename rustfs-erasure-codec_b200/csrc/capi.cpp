@@ -155,6 +155,37 @@ int do_reconstruct(Codec &c, size_t n, uint8_t *const *sh, const uint8_t *presen
 // Which shards a stripe reads (in) and writes (out) for an operation.
 enum Op { OP_ENCODE, OP_VERIFY, OP_RECONSTRUCT };
 
+// Queues shard copies in one direction on one stream, merging copies that are
+// contiguous on both sides into a single cudaMemcpyAsync: a stripe's shards,
+// and consecutive stripes, usually sit back to back in the caller's buffer and
+// in the staging area, so a chunk moves in a few large transfers.
+struct CopyRun {
+  cudaMemcpyKind kind;
+  cudaStream_t s;
+  char *dst = nullptr;
+  const char *src = nullptr;
+  size_t bytes = 0;
+  int add(void *d, const void *from, size_t n) {
+    char *dd = static_cast<char *>(d);
+    const char *ss = static_cast<const char *>(from);
+    if (bytes && dd == dst + bytes && ss == src + bytes) {
+      bytes += n;
+      return RSGPU_OK;
+    }
+    const int rc = flush();
+    dst = dd;
+    src = ss;
+    bytes = n;
+    return rc;
+  }
+  int flush() {
+    if (!bytes) return RSGPU_OK;
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, s);
+    bytes = 0;
+    return e == cudaSuccess ? RSGPU_OK : rsgpu::cuda_status(e);
+  }
+};
+
 // Host-memory execution: stage chunks of stripes through device memory.
 // `in_mask`/`out_mask` (per stripe, k+m flags) say which shards to copy in
 // and back.
@@ -187,14 +218,15 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
     for (size_t i = 0; i < cnt * total; ++i) dptr[i] = stage + i * pitch;
     // Inputs are queued first; the job-table upload and the kernel follow them
     // on the same stream.
+    CopyRun up{cudaMemcpyHostToDevice, s};
     for (size_t sidx = 0; sidx < cnt; ++sidx) {
       const size_t st = base + sidx;
       for (size_t i = 0; i < total; ++i) {
         bool in = op == OP_ENCODE ? i < c.k : op == OP_VERIFY ? true : present[st * total + i] != 0;
-        if (in)
-          RS_CUDA(cudaMemcpyAsync(dptr[sidx * total + i], host[st * total + i], len, cudaMemcpyHostToDevice, s));
+        if (in && (rc = up.add(dptr[sidx * total + i], host[st * total + i], len))) return rc;
       }
     }
+    if ((rc = up.flush())) return rc;
     if (op == OP_ENCODE)
       status = do_encode(c, cnt, dptr.data(), len, s);
     else if (op == OP_VERIFY)
@@ -202,6 +234,7 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
     else
       status = do_reconstruct(c, cnt, dptr.data(), present + base * total, len, goal, req, nreq, s);
     if (status == RSGPU_OK && op != OP_VERIFY) {
+      CopyRun down{cudaMemcpyDeviceToHost, s};
       for (size_t sidx = 0; sidx < cnt; ++sidx) {
         const size_t st = base + sidx;
         const uint8_t *pr = op == OP_RECONSTRUCT ? present + st * total : nullptr;
@@ -214,10 +247,10 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
             out = !pr[i] && (goal == RSGPU_GOAL_ALL || (goal == RSGPU_GOAL_DATA && i < c.k) ||
                              (goal == RSGPU_GOAL_REQUIRED && i < nreq && req[i]));
           }
-          if (out)
-            RS_CUDA(cudaMemcpyAsync(host[st * total + i], dptr[sidx * total + i], len, cudaMemcpyDeviceToHost, s));
+          if (out && (rc = down.add(host[st * total + i], dptr[sidx * total + i], len))) return rc;
         }
       }
+      if ((rc = down.flush())) return rc;
     }
     RS_CUDA(cudaFreeAsync(stage, s));
   }
