@@ -256,6 +256,7 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
   }
   RS_CUDA(cudaStreamSynchronize(h->io[0]));
   RS_CUDA(cudaStreamSynchronize(h->io[1]));
+  if (status == RSGPU_OK) status = c.take_device_status(h->io[0]);
   return status;
 }
 
@@ -586,6 +587,7 @@ int32_t rsgpu_batch_prepare(const rsgpu_codec *hc, int32_t op, size_t n_stripes,
       rc = c.encode_jobs(n_stripes, ptrs, jobs, dptrs, op == RSGPU_OP_VERIFY);
     }
     if (rc == RSGPU_OK) rc = b->apply.build(jobs, dptrs, len, op == RSGPU_OP_VERIFY, b->flags, nullptr, true);
+    b->apply.args.stall = c.d_status;
   }
   if (rc) return rc;
   *out = b.release();

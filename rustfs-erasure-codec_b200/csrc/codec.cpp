@@ -86,6 +86,18 @@ Codec::~Codec() {
   if (d_log) cudaFree(d_log);
   if (d_exp) cudaFree(d_exp);
   if (d_enc_tbl) cudaFree(d_enc_tbl);
+  if (d_status) cudaFree(d_status);
+}
+
+int Codec::take_device_status(cudaStream_t s) {
+  if (!d_status) return RSGPU_OK;
+  uint32_t v = 0;
+  RS_CUDA(cudaMemcpyAsync(&v, d_status, 4, cudaMemcpyDeviceToHost, s));
+  RS_CUDA(cudaStreamSynchronize(s));
+  if (!v) return RSGPU_OK;
+  RS_CUDA(cudaMemsetAsync(d_status, 0, 4, s));
+  RS_CUDA(cudaStreamSynchronize(s));
+  return RSGPU_ERR_DEVICE_TIMEOUT;
 }
 
 int Codec::init_classic(const uint8_t *custom_rows) {
@@ -103,6 +115,8 @@ int Codec::init_classic(const uint8_t *custom_rows) {
   pack_tables(&matrix[k * k], m, k, packed.data());
   RS_CUDA(cudaMalloc(&d_enc_tbl, packed.size() * 4));
   RS_CUDA(cudaMemcpy(d_enc_tbl, packed.data(), packed.size() * 4, cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMalloc(&d_status, 4));
+  RS_CUDA(cudaMemset(d_status, 0, 4));
   pool_.reset(new TablePool(std::max<size_t>(256, packed_table_words(m, k) * 4)));
   // Distinct patterns are unbounded in number, but decode tables are small:
   // keep up to 65536 resident unless the caller set an explicit capacity.
@@ -379,6 +393,7 @@ int Codec::run_apply(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &p
   ApplyLaunch l;
   int rc = l.build(jobs, ptrs, len, verify, flags_dev, s, false, accumulate);
   if (rc) return rc;
+  l.args.stall = d_status;
   rc = l.launch(s);
   l.release(s);
   return rc;
@@ -419,7 +434,7 @@ int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len
   std::vector<uint32_t> f(n_stripes);
   RS_CUDA(cudaMemcpyAsync(f.data(), flags, n_stripes * 4, cudaMemcpyDeviceToHost, s));
   RS_CUDA(cudaFreeAsync(flags, s));
-  RS_CUDA(cudaStreamSynchronize(s));
+  if ((rc = take_device_status(s))) return rc;  // also waits for s
   for (size_t i = 0; i < n_stripes; ++i) ok_host[i] = f[i] ? 0 : 1;
   return RSGPU_OK;
 }

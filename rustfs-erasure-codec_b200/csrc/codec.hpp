@@ -107,11 +107,17 @@ class Codec {
   uint8_t *d_matrix = nullptr;
   uint8_t *d_log = nullptr, *d_exp = nullptr;
   uint32_t *d_enc_tbl = nullptr;  // parity rows packed for K1
+  // Set by a K1 launch whose bounded device wait ran out; read and cleared
+  // by the next synchronous call (take_device_status).
+  uint32_t *d_status = nullptr;
   std::shared_ptr<LeopardState> leo;  // created where the type is complete
   std::shared_ptr<TowerState> tower;
 
   ~Codec();
   int init_classic(const uint8_t *custom_rows);
+  // RSGPU_ERR_DEVICE_TIMEOUT (and clears it) when a launch of this codec
+  // recorded a stalled wait; waits for stream s.
+  int take_device_status(cudaStream_t s);
   int init_tower(const uint8_t *custom_rows);
   int init_leopard();
 

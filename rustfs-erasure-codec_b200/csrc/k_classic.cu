@@ -23,16 +23,11 @@ namespace rsgpu {
 
 namespace {
 
-// L2 prefetch of `bytes` (a multiple of 16) at a 16-byte-aligned address.
-__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// Grid-stride loop of apply_tile over every (job, tile) of a launch.  With
-// PF, the CTA first asks L2 for the input columns of the tile it will take
-// next (one bulk prefetch per input shard), so those loads are L2 hits.
-template <int NG, int V, int kBatch, int MIX, bool VERIFY, bool PF = false, int MINB = 0, bool ACC = false>
-__global__ void __launch_bounds__(kApplyThreads, MINB ? MINB : ((NG == 1 && V <= 2) ? 4 : 1)) k_apply_vec(ApplyArgs a) {
+// Grid-stride loop of apply_tile over every (job, tile) of a launch, inputs
+// loaded straight into registers: the tile for more than 4 outputs and for
+// accumulating (incremental parity) launches.
+template <int NG, int V, int kBatch, int MIX, bool VERIFY, bool ACC = false>
+__global__ void __launch_bounds__(kApplyThreads, (NG == 1 && V <= 2) ? 4 : 1) k_apply_vec(ApplyArgs a) {
   constexpr uint32_t kTile = kApplyThreads * kApplyVec * V;
   const uint32_t tiles_per_job = uint32_t((a.len + kTile - 1) / kTile);
   const uint32_t total = tiles_per_job * a.n_jobs;
@@ -40,20 +35,201 @@ __global__ void __launch_bounds__(kApplyThreads, MINB ? MINB : ((NG == 1 && V <=
     const uint32_t job = t / tiles_per_job;
     const uint64_t tile_base = uint64_t(t - job * tiles_per_job) * kTile;
     const JobDesc d = a.jobs[job];
-    if (PF) {
-      const uint32_t t2 = t + gridDim.x;
-      if (t2 < total) {
-        const uint32_t job2 = t2 / tiles_per_job;
-        const uint64_t base2 = uint64_t(t2 - job2 * tiles_per_job) * kTile;
-        const JobDesc d2 = a.jobs[job2];
-        if (threadIdx.x < d2.n_in && base2 < d2.vec_len) {
-          const uint64_t left = d2.vec_len - base2;
-          prefetch_l2(a.ptrs[d2.ptr_off + threadIdx.x] + base2, uint32_t(left < kTile ? left : kTile));
-        }
-      }
-    }
     if (tile_base >= d.vec_len) continue;  // CTA-uniform
     apply_tile<NG, V, kBatch, MIX, VERIFY, ACC>(a.ptrs, a.flags, d, tile_base);
+  }
+}
+
+// ------------------------------------------------------------------ K1, TMA-staged
+// The same product as k_apply_vec<1, V, 4, 0> with the input tiles staged in
+// shared memory by the bulk-copy (TMA) unit: one producer warp streams each
+// step's tile slices (one contiguous 256 * 16 * V-byte slice per input shard,
+// cp.async.bulk with completion on the stage's mbarrier) into a ring of S
+// stages of 4 slots; kApplyThreads consumer threads wait for a stage, run the
+// table arithmetic from shared memory and release it.  A step is up to 4
+// input shards of one tile, or for verify the tile's <= 4 parity shards.
+// n_out <= 4 only.  Every wait is bounded (about 2 s of SM clock); a wait
+// that runs out sets *a.stall (the codec's status word, read back by the
+// next synchronous call as RSGPU_ERR_DEVICE_TIMEOUT), and the producer then
+// waits, bounded again, for the copies it has in flight before it exits.
+// Measured against the register-path tile (k_apply_vec<1, 2, 4, 0>) on
+// 1024 x 1 MiB stripes: 10+4 encode 4650 vs 4268 GB/s; global-load stalls per
+// issued instruction fall from 4.1 to 1.7, and the bulk copies do not compete
+// with the table shuffles for the L1 data pipe (cp.async staging, which
+// does, was 7-14% slower than the register path).
+constexpr long long kStallCycles = 4000000000ll;
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// Wait for the completion of the barrier phase with this parity; false when
+// the wait ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > kStallCycles) return false;
+  }
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ uint4 lds128(uint32_t addr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr)
+               : "memory");
+  return v;
+}
+
+template <int V, int S, bool VERIFY>
+__global__ void __launch_bounds__(kApplyThreads + 32, 2) k_apply_tma(ApplyArgs a) {
+  constexpr uint32_t kSlot = kApplyThreads * kApplyVec * V;  // one input's slice of a tile
+  extern __shared__ __align__(128) uint8_t tma_smem[];
+  __shared__ __align__(8) uint64_t full[S], empty[S];
+  const uint32_t tid = threadIdx.x, lane = tid & 31;
+  const uint32_t sbase = uint32_t(__cvta_generic_to_shared(tma_smem));
+  const uint32_t fbar = uint32_t(__cvta_generic_to_shared(full));
+  const uint32_t ebar = uint32_t(__cvta_generic_to_shared(empty));
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(fbar + 8 * s, 1);
+      mbar_init(ebar + 8 * s, kApplyThreads / 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const uint32_t tiles_per_job = uint32_t((a.len + kSlot - 1) / kSlot);
+  const uint32_t total = tiles_per_job * a.n_jobs;
+
+  if (tid >= kApplyThreads) {  // producer warp: one lane issues every copy
+    if (tid != kApplyThreads) return;
+    uint32_t it = 0;
+    bool ok = true;
+    for (uint32_t t = blockIdx.x; t < total && ok; t += gridDim.x) {
+      const uint32_t job = t / tiles_per_job;
+      const uint64_t base = uint64_t(t - job * tiles_per_job) * kSlot;
+      const JobDesc d = a.jobs[job];
+      if (base >= d.vec_len) continue;
+      const uint32_t valid = uint32_t(d.vec_len - base < kSlot ? d.vec_len - base : kSlot);
+      const uint8_t *const *ptr = a.ptrs + d.ptr_off;
+      const uint32_t steps = (d.n_in + 3) / 4 + (VERIFY ? 1 : 0);
+      for (uint32_t step = 0; step < steps; ++step, ++it) {
+        const uint32_t s = it % S, ph = (it / S) & 1;
+        if (!mbar_wait(ebar + 8 * s, ph ^ 1)) {
+          ok = false;
+          break;
+        }
+        const bool par = VERIFY && step * 4 >= d.n_in;
+        const uint32_t j0 = par ? d.n_in : step * 4;
+        const uint32_t rows = par ? d.n_out : min(4u, d.n_in - j0);
+        mbar_expect_tx(fbar + 8 * s, rows * valid);
+        for (uint32_t b = 0; b < rows; ++b)
+          bulk_load(sbase + (s * 4 + b) * kSlot, ptr[j0 + b] + base, valid, fbar + 8 * s);
+      }
+    }
+    if (!ok) {
+      if (a.stall) atomicOr(a.stall, 1u);
+      // Copies already issued land in stages the consumers stopped reading:
+      // wait (bounded) for them before the CTA's shared memory goes away.
+      for (uint32_t k = 0; k < S && k < it; ++k) {
+        const uint32_t i = it - 1 - k;
+        mbar_wait(fbar + 8 * (i % S), (i / S) & 1);
+      }
+    }
+    return;
+  }
+
+  // Consumers: the same (tile, step) sequence as the producer.
+  uint32_t it = 0;
+  for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+    const uint32_t job = t / tiles_per_job;
+    const uint64_t base = uint64_t(t - job * tiles_per_job) * kSlot;
+    const JobDesc d = a.jobs[job];
+    if (base >= d.vec_len) continue;
+    const uint32_t n_in = d.n_in;
+    const uint32_t steps = (n_in + 3) / 4 + (VERIFY ? 1 : 0);
+    uint64_t col[V];
+    bool active[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      col[v] = base + (uint64_t(v) * kApplyThreads + tid) * kApplyVec;
+      active[v] = col[v] < d.vec_len;
+    }
+    uint32_t acc[V][16];
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+#pragma unroll
+      for (int i = 0; i < 16; ++i) acc[v][i] = 0;
+    bool bad = false;
+    for (uint32_t step = 0; step < steps; ++step, ++it) {
+      const uint32_t s = it % S, ph = (it / S) & 1;
+      if (!mbar_wait(fbar + 8 * s, ph)) {
+        if (a.stall) atomicOr(a.stall, 1u);
+        return;
+      }
+      const uint32_t slot0 = sbase + s * 4 * kSlot + tid * kApplyVec;
+      const bool par = VERIFY && step * 4 >= n_in;
+      if (!par) {
+        const uint32_t j0 = step * 4;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          if (j0 + b >= n_in) break;  // warp-uniform
+          const uint32_t *tb = d.tbl + (j0 + b) * kTableWords;
+          const uint32_t lo = __ldg(tb + (lane & 15));
+          const uint32_t hi = __ldg(tb + 16 + (lane & 15));
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const uint4 x = lds128(slot0 + b * kSlot + v * kApplyThreads * kApplyVec);
+            mac4(x.x, lo, hi, &acc[v][0]);
+            mac4(x.y, lo, hi, &acc[v][4]);
+            mac4(x.z, lo, hi, &acc[v][8]);
+            mac4(x.w, lo, hi, &acc[v][12]);
+          }
+        }
+      }
+      if (step + 1 == steps) {  // outputs of this tile (parity rows are in this stage when VERIFY)
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          uint32_t o[4][4];
+#pragma unroll
+          for (int w = 0; w < 4; ++w) {
+            uint32_t tmp[4];
+            transpose4(&acc[v][w * 4], tmp);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) o[r][w] = tmp[r];
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            if (uint32_t(r) < d.n_out && active[v]) {
+              if (VERIFY) {
+                const uint4 e = lds128(slot0 + r * kSlot + v * kApplyThreads * kApplyVec);
+                bad |= (e.x != o[r][0]) | (e.y != o[r][1]) | (e.z != o[r][2]) | (e.w != o[r][3]);
+              } else {
+                uint8_t *dst = const_cast<uint8_t *>(a.ptrs[d.ptr_off + n_in + r]) + col[v];
+                st_stream(dst, make_uint4(o[r][0], o[r][1], o[r][2], o[r][3]));
+              }
+            }
+          }
+        }
+        if (VERIFY && __any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flags + d.flag_idx, 1u);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(ebar + 8 * s);
+    }
   }
 }
 
@@ -199,15 +375,29 @@ int grid_for(const void *fn, int threads, size_t smem) {
   return sms * per_sm;
 }
 
-template <int NG, int V, int B, int MIX, bool VERIFY, bool PF = false, int MINB = 0, bool ACC = false>
+template <int NG, int V, int B, int MIX, bool VERIFY, bool ACC = false>
 void launch_vec(const ApplyArgs &a, cudaStream_t s) {
   static int grid_max = 0;
-  if (!grid_max)
-    grid_max = grid_for((const void *)k_apply_vec<NG, V, B, MIX, VERIFY, PF, MINB, ACC>, kApplyThreads, 0);
+  if (!grid_max) grid_max = grid_for((const void *)k_apply_vec<NG, V, B, MIX, VERIFY, ACC>, kApplyThreads, 0);
   const uint64_t tile = uint64_t(kApplyThreads) * kApplyVec * V;
   const uint64_t tiles = ((a.len + tile - 1) / tile) * a.n_jobs;
   const int grid = int(tiles < uint64_t(grid_max) ? tiles : grid_max);
-  k_apply_vec<NG, V, B, MIX, VERIFY, PF, MINB, ACC><<<grid, kApplyThreads, 0, s>>>(a);
+  k_apply_vec<NG, V, B, MIX, VERIFY, ACC><<<grid, kApplyThreads, 0, s>>>(a);
+}
+
+template <int V, int S, bool VERIFY>
+void launch_tma(const ApplyArgs &a, cudaStream_t s) {
+  constexpr size_t smem = size_t(S) * 4 * kApplyThreads * kApplyVec * V;
+  static int grid_max = 0;
+  if (!grid_max) {
+    const void *fn = (const void *)k_apply_tma<V, S, VERIFY>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    grid_max = grid_for(fn, kApplyThreads + 32, smem);
+  }
+  const uint64_t tile = uint64_t(kApplyThreads) * kApplyVec * V;
+  const uint64_t tiles = ((a.len + tile - 1) / tile) * a.n_jobs;
+  const int grid = int(tiles < uint64_t(grid_max) ? tiles : grid_max);
+  k_apply_tma<V, S, VERIFY><<<grid, kApplyThreads + 32, smem, s>>>(a);
 }
 
 // Tile variants the autotuner chooses from: (vectors per thread, inputs in
@@ -219,21 +409,10 @@ void launch_variant(const ApplyArgs &a, int variant, cudaStream_t s) {
     return;
   }
   switch (variant) {
-    case 0: launch_vec<1, 2, 4, 0, VERIFY>(a, s); break;
-    case 2: launch_vec<1, 2, 4, 2, VERIFY>(a, s); break;
-    case 3: launch_vec<1, 1, 8, 1, VERIFY>(a, s); break;
-    case 4: launch_vec<1, 1, 4, 1, VERIFY>(a, s); break;
-    case 1: launch_vec<1, 2, 4, 1, VERIFY>(a, s); break;
-    case 5: launch_vec<1, 2, 4, 0, VERIFY, true>(a, s); break;
-    case 6: launch_vec<1, 1, 8, 0, VERIFY>(a, s); break;
-    case 7: launch_vec<1, 1, 8, 0, VERIFY, true>(a, s); break;
-    case 8: launch_vec<1, 4, 2, 0, VERIFY>(a, s); break;
-    case 9: launch_vec<1, 2, 2, 0, VERIFY, true>(a, s); break;
-    case 10: launch_vec<1, 1, 4, 0, VERIFY, false, 6>(a, s); break;
-    case 11: launch_vec<1, 1, 2, 0, VERIFY, false, 8>(a, s); break;
-    case 12: launch_vec<1, 2, 2, 0, VERIFY, false, 6>(a, s); break;
-    case 13: launch_vec<1, 1, 4, 0, VERIFY, false, 4>(a, s); break;
-    default: launch_vec<1, 2, 4, 0, VERIFY>(a, s); break;
+    case 1: launch_vec<1, 2, 4, 0, VERIFY>(a, s); break;  // register path
+    case 2: launch_tma<2, 2, VERIFY>(a, s); break;
+    case 3: launch_tma<1, 4, VERIFY>(a, s); break;
+    default: launch_tma<2, 3, VERIFY>(a, s); break;  // 0: TMA-staged, 2 x 16 B per thread, 3 stages
   }
 }
 
@@ -252,7 +431,7 @@ cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cud
   uint64_t launches = 0;
   if (a.any_vec && a.len >= 16) {
     if (a.accumulate)
-      launch_vec<1, 2, 4, 0, false, false, 0, true>(a, s);
+      launch_vec<1, 2, 4, 0, false, true>(a, s);
     else if (verify)
       launch_variant<true>(a, apply_variant(), s);
     else

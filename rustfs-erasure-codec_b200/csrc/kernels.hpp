@@ -17,10 +17,12 @@ struct ApplyArgs {
   uint32_t max_out;             // largest n_out over the jobs
   int any_vec;                  // some job has vec_len > 0
   int accumulate;               // outputs ^= products (incremental parity update)
+  uint32_t *stall;              // device status word: a bounded wait of the TMA-staged tile ran out (may be null)
 };
 cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cudaStream_t s);
-// K1 tile variant (threads x vectors-per-thread x inputs-in-flight); the
-// autotuner sets it, RSGPU_APPLY_VARIANT overrides the default.
+// K1 tile for launches of at most 4 outputs: 0 (default) TMA-staged, 1 the
+// register-path tile, 2 / 3 other TMA ring shapes; RSGPU_APPLY_VARIANT picks
+// one for measurements.
 int &apply_variant();
 
 // K3: one erasure pattern.  Indices fit a byte because classic codecs have at
