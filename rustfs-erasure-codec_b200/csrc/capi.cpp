@@ -73,6 +73,32 @@ int ensure_io(rsgpu_codec *h) {
 
 size_t round16(size_t n) { return (n + 15) & ~size_t(15); }
 
+// Staging memory of host-memory calls comes from a pool private to this
+// library (one per device), which keeps up to 1 GiB of freed memory mapped
+// between calls: the device's default pool gives freed memory back at every
+// synchronisation, so each call would map its staging area afresh.  A private
+// pool leaves the default pool's settings (which other code in the process
+// may rely on) untouched.
+int staging_pool(int device, cudaMemPool_t *out) {
+  static std::mutex mu;
+  static std::vector<cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> g(mu);
+  if (pools.size() <= size_t(device)) pools.resize(size_t(device) + 1, nullptr);
+  if (!pools[device]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t p = nullptr;
+    RS_CUDA(cudaMemPoolCreate(&p, &props));
+    uint64_t keep = 1ull << 30;
+    RS_CUDA(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[device] = p;
+  }
+  *out = pools[device];
+  return RSGPU_OK;
+}
+
 // Stripes per host-staging chunk: about 256 MiB of device staging each.
 size_t chunk_stripes(size_t per_stripe_bytes) {
   size_t c = (256u << 20) / std::max<size_t>(per_stripe_bytes, 1);
@@ -205,6 +231,8 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
   cudaEventDestroy(ev);
   const size_t pitch = round16(len);
   const size_t per = chunk_stripes(total * pitch);
+  cudaMemPool_t pool = nullptr;
+  if ((rc = staging_pool(c.device, &pool))) return rc;
   std::vector<uint8_t *> dptr;
   std::vector<uint8_t> in_flags(total), out_flags(total);
   int status = RSGPU_OK;
@@ -212,7 +240,7 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
     const size_t cnt = std::min(per, n_stripes - base);
     cudaStream_t s = h->io[ci & 1];
     uint8_t *stage = nullptr;
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&stage), cnt * total * pitch, s);
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&stage), cnt * total * pitch, pool, s);
     if (e != cudaSuccess) return rsgpu::cuda_status(e);
     dptr.resize(cnt * total);
     for (size_t i = 0; i < cnt * total; ++i) dptr[i] = stage + i * pitch;
