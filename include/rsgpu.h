@@ -483,6 +483,7 @@ typedef struct rsgpu_server_stats {
   uint64_t submitted, completed, launches;
   size_t pending, inflight, budget_bytes, reserved_bytes, max_reserved_bytes;
   uint32_t max_concurrent_launches, pad;
+  double prepare_seconds; /* worker time spent planning, building and launching batches */
 } rsgpu_server_stats;
 void rsgpu_server_options_default(rsgpu_server_options *out);
 int32_t rsgpu_server_new(const rsgpu_server_options *opts, rsgpu_server **out);

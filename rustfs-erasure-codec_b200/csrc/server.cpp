@@ -179,6 +179,7 @@ class Server {
     s->reserved_bytes = reserved_;
     s->max_reserved_bytes = max_reserved_;
     s->max_concurrent_launches = max_concurrent_;
+    s->prepare_seconds = prepare_s_;
   }
 
  private:
@@ -194,6 +195,7 @@ class Server {
   uint64_t submitted_ = 0, completed_ = 0, launches_ = 0;
   size_t inflight_ = 0, reserved_ = 0, max_reserved_ = 0;
   uint32_t max_concurrent_ = 0;
+  double prepare_s_ = 0;  // worker time spent building and launching batches
   Clock::time_point t0_;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0_).count(); }
@@ -287,6 +289,15 @@ class Server {
     }
     if (take.empty()) return false;
     const double t = now();
+    struct Timer {  // adds this call's host time to prepare_s_ on every return path
+      Server *sv;
+      double t0;
+      ~Timer() {
+        const double dt = sv->now() - t0;
+        std::lock_guard<std::mutex> g(sv->mu_);
+        sv->prepare_s_ += dt;
+      }
+    } timer{this, t};
     std::vector<size_t> in, out;
     std::vector<rsgpu_mix_op> ops(take.size());
     int rc = RSGPU_OK;

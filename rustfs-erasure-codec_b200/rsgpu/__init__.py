@@ -128,7 +128,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("launches", ctypes.c_uint64),
                 ("pending", ctypes.c_size_t), ("inflight", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t),
                 ("reserved_bytes", ctypes.c_size_t), ("max_reserved_bytes", ctypes.c_size_t),
-                ("max_concurrent_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+                ("max_concurrent_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+                ("prepare_seconds", ctypes.c_double)]
 
 
 class StreamOptions(ctypes.Structure):
