@@ -533,8 +533,7 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
           for (uint16_t x : mp.inputs) B.ptrs.push_back(o.shards[x]);
           for (uint16_t t : mp.targets) B.ptrs.push_back(o.shards[t]);
           const size_t toff = B.tables.size();
-          B.tables.resize(toff + packed_table_words(mp.targets.size(), mp.inputs.size()));
-          pack_tables_with(leopard_mul8(), mp.rows.data(), mp.targets.size(), mp.inputs.size(), B.tables.data() + toff);
+          B.tables.insert(B.tables.end(), mp.packed->begin(), mp.packed->end());  // packed once per pattern
           add_apply_job(B, p, false, mp.inputs.size(), mp.targets.size(), off, len, 0, nullptr, toff);
           B.algorithmic_bytes += uint64_t(mp.inputs.size() + mp.targets.size()) * len;
         }

@@ -463,6 +463,19 @@ int Codec::apply_parity_columns(const std::vector<const uint8_t *> &inputs, cons
   return rc;
 }
 
+int Codec::apply_with_tables(std::vector<JobDesc> &jobs, const std::vector<size_t> &tbl_off,
+                             std::vector<const uint8_t *> &ptrs, const std::vector<uint32_t> &tables, size_t len,
+                             cudaStream_t s) {
+  if (jobs.empty()) return RSGPU_OK;
+  void *d = nullptr;
+  int rc = upload(tables.data(), tables.size() * 4, &d, s);
+  if (rc) return rc;
+  for (size_t i = 0; i < jobs.size(); ++i) jobs[i].tbl = static_cast<const uint32_t *>(d) + tbl_off[i];
+  rc = run_apply(jobs, ptrs, len, false, nullptr, s);
+  RS_CUDA(cudaFreeAsync(d, s));
+  return rc;
+}
+
 int Codec::verify_dev_async(size_t n_stripes, uint8_t *const *shards, size_t len, uint32_t *flags_dev,
                             cudaStream_t s) {
   std::vector<JobDesc> jobs;

@@ -142,6 +142,13 @@ class Codec {
   int apply_parity_columns(const std::vector<const uint8_t *> &inputs, const std::vector<size_t> &cols,
                            uint8_t *const *parity, size_t len, bool accumulate, cudaStream_t s);
 
+  // K1 over jobs whose packed tables are given on the host: `tables` is
+  // uploaded stream-ordered, job i reads it from word tbl_off[i]; device
+  // pointers in `ptrs`.
+  int apply_with_tables(std::vector<JobDesc> &jobs, const std::vector<size_t> &tbl_off,
+                        std::vector<const uint8_t *> &ptrs, const std::vector<uint32_t> &tables, size_t len,
+                        cudaStream_t s);
+
   // Decode tables for a set of plans, building missing entries on the GPU (K3).
   int decode_tables(const std::vector<const ClassicPlan *> &plans, std::vector<const uint32_t *> &tbls,
                     cudaStream_t s);

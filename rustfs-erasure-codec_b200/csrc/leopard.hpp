@@ -61,10 +61,13 @@ int leopard_dense_encode(Codec &c, std::vector<uint8_t> &rows);
 // The GF(2^8) Leopard reconstruction of one presence pattern as a dense map
 // from the present shards (ascending) to the targets (ascending).  The
 // reference's decode uses every present shard, and so does this map, so the
-// bytes agree on any input, codeword or not.
+// bytes agree on any input, codeword or not.  Maps (with their K1 tables) are
+// cached per codec by (pattern, goal), least recently used first out beyond
+// 64 MiB; GF(2^8) per-call reconstructs run them through K1.
 struct LeoDenseMap {
   std::vector<uint16_t> inputs, targets;
   std::vector<uint8_t> rows;  // targets x inputs
+  std::shared_ptr<const std::vector<uint32_t>> packed;  // rows packed for K1 (Leopard multiplication)
 };
 int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, std::vector<LeoDenseMap> &maps,
                          cudaStream_t s);

@@ -191,6 +191,72 @@ def test_lgf16_wide_decode_matches_oracle(rs, torch, k, m, size, codeword):
             assert np.array_equal(lst[i].cpu().numpy(), ref[i]), (k, m, e, i)
 
 
+@pytest.mark.parametrize("k,m", [(4, 2), (32, 16), (128, 64)])
+def test_lgf8_dense_reconstruct_matches_oracle(rs, torch, k, m):
+    # GF(2^8) reconstructs of shards >= 32 KiB with <= 16 targets run the
+    # pattern's dense map through K1 (wider maps on short shards run the FFT
+    # decode); arbitrary (non-codeword) inputs pin both to the reference.
+    size = 65536 + 3 * 64  # Leopard shards are 64-byte multiples
+    rng = np.random.default_rng(k * 31 + m)
+    full = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k + m)]
+    c = codec(rs, 8, k, m)
+    for e, goal in ((m, "all"), (min(16, max(1, m // 3)), "all"), (min(16, m), "data")):
+        lost = set(rng.choice(k + m, size=e, replace=False).tolist())
+        pres = [0 if i in lost else 1 for i in range(k + m)]
+        ref = [s.copy() for s in full]
+        for i in lost:
+            ref[i][:] = 0
+        assert O.leopard_reconstruct(8, k, m, ref, pres) == 0
+        buf = torch.from_numpy(np.stack(full)).cuda()
+        lst = [None if i in lost else buf[i] for i in range(k + m)]
+        (c.reconstruct if goal == "all" else c.reconstruct_data)(lst)
+        for i in sorted(lost):
+            if goal == "data" and i >= k:
+                assert lst[i] is None
+            else:
+                assert np.array_equal(lst[i].cpu().numpy(), ref[i]), (k, m, e, goal, i)
+        # The same pattern on short shards: a cached map also runs dense.
+        short = [s[:64].copy() for s in full]
+        sref = [s[:64].copy() for s in ref]
+        sbuf = torch.from_numpy(np.stack(short)).cuda()
+        slst = [None if i in lost else sbuf[i] for i in range(k + m)]
+        (c.reconstruct if goal == "all" else c.reconstruct_data)(slst)
+        for i in sorted(lost):
+            if not (goal == "data" and i >= k):
+                assert np.array_equal(slst[i].cpu().numpy(), sref[i]), (k, m, e, goal, i, "short")
+
+
+def test_lgf8_dense_batch_of_mixed_patterns(rs, torch):
+    # Several stripes, several patterns (one repeated, one stripe with nothing
+    # to do) in one host-memory batch call.
+    k, m, size, n = 32, 16, 40960, 6
+    rng = np.random.default_rng(77)
+    c = codec(rs, 8, k, m)
+    stripes, pats, refs = [], [], []
+    for s in range(n):
+        full = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k + m)]
+        e = 0 if s == 3 else int(rng.integers(1, m + 1))
+        lost = set(rng.choice(k + m, size=e, replace=False).tolist()) if e else set()
+        if s == 5:
+            lost = {i for i, p in enumerate(pats[1]) if not p}  # repeats stripe 1's pattern
+        pres = [0 if i in lost else 1 for i in range(k + m)]
+        ref = [x.copy() for x in full]
+        for i in lost:
+            ref[i][:] = 0
+        if lost:
+            assert O.leopard_reconstruct(8, k, m, ref, pres) == 0
+        work = [x.copy() for x in full]
+        for i in lost:
+            work[i][:] = 0x5A
+        stripes.append(work)
+        pats.append(pres)
+        refs.append(ref)
+    c.reconstruct_batch(stripes, pats)
+    for s in range(n):
+        for i in range(k + m):
+            assert np.array_equal(stripes[s][i], refs[s][i]), (s, i)
+
+
 def test_leopard_errors(rs, torch):
     c = codec(rs, 8, 4, 2)
     sh = [torch.zeros(100, dtype=torch.uint8, device="cuda") for _ in range(6)]
