@@ -36,13 +36,19 @@ struct UploadSlot {
     if (host) cudaFreeHost(host);
   }
 };
-thread_local UploadSlot t_upload;
+// A small ring per thread, so an upload waits only for the copy issued
+// kUploadSlots uploads earlier (a call that uploads tables and then its job
+// blob does not wait for its own first copy).
+constexpr int kUploadSlots = 4;
+thread_local UploadSlot t_upload[kUploadSlots];
+thread_local int t_upload_next = 0;
 
 // Copies `bytes` of host data to a fresh stream-ordered device allocation
 // through a pinned, event-guarded bounce buffer.  The device block is freed
 // stream-ordered by the caller.
 int upload(const void *src, size_t bytes, void **dev, cudaStream_t s) {
-  UploadSlot &u = t_upload;
+  UploadSlot &u = t_upload[t_upload_next];
+  t_upload_next = (t_upload_next + 1) % kUploadSlots;
   if (!u.done) RS_CUDA(cudaEventCreateWithFlags(&u.done, cudaEventDisableTiming));
   RS_CUDA(cudaEventSynchronize(u.done));  // previous upload from this thread has left the buffer
   if (u.cap < bytes) {

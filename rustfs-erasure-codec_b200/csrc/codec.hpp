@@ -142,6 +142,11 @@ class Codec {
   int apply_parity_columns(const std::vector<const uint8_t *> &inputs, const std::vector<size_t> &cols,
                            uint8_t *const *parity, size_t len, bool accumulate, cudaStream_t s);
 
+  // K1 over jobs whose `tbl` pointers already point at device tables.
+  int apply_jobs(std::vector<JobDesc> &jobs, std::vector<const uint8_t *> &ptrs, size_t len, cudaStream_t s) {
+    return run_apply(jobs, ptrs, len, false, nullptr, s);
+  }
+
   // K1 over jobs whose packed tables are given on the host: `tables` is
   // uploaded stream-ordered, job i reads it from word tbl_off[i]; device
   // pointers in `ptrs`.

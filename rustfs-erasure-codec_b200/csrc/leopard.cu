@@ -356,6 +356,7 @@ struct LeopardState {
   cudaEvent_t scratch_done = nullptr;
   std::mutex scratch_mu;
   std::vector<uint8_t> dense_enc;  // GF(2^8): the encode map as an m x k matrix
+  uint32_t *d_dense_enc = nullptr;  // ... packed for K1, device-resident (filled with dense_enc)
   // GF(2^8) decode maps by (presence pattern, goal), with their K1 tables,
   // least recently used first out beyond kDenseCacheBytes (under mu).
   struct DenseEntry {
@@ -371,6 +372,7 @@ struct LeopardState {
     for (void *p : plan_slabs) cudaFree(p);
     if (scratch) cudaFree(scratch);
     for (void *p : owned) cudaFree(p);
+    if (d_dense_enc) cudaFree(d_dense_enc);
     if (scratch_done) cudaEventDestroy(scratch_done);
   }
 };
@@ -924,7 +926,36 @@ static int run_once(Codec &c, int op, size_t n, uint8_t *const *shards, const ui
   return leo_launch(L, s);
 }
 
+// GF(2^8) codes with at most 4 parity shards encode shards of 128 KiB and
+// more through K1 with the codec's dense encode map (the FFT encode's own
+// linear map, so the same bytes; its packed tables stay on the device):
+// per call, 10+4 at 1 MiB 1.3x and at 4 MiB 1.6x faster than the FFT encode
+// (the kernels alone: 3.1 against 0.54 TB/s).  Below 128 KiB the FFT call's
+// smaller host cost wins; with more parity the transform is as fast (32+16)
+// or much faster (128+64), so it stays.
+constexpr size_t kDenseEncMinLen = size_t(128) << 10;
+
 int leopard_encode(Codec &c, size_t n, uint8_t *const *shards, size_t len, cudaStream_t s) {
+  if (c.leo->field->bits == 8 && c.m <= 4 && len >= kDenseEncMinLen && n > 0) {
+    std::vector<uint8_t> rows;
+    int rc = leopard_dense_encode(c, rows);
+    if (rc) return rc;
+    const uint32_t *tbl = nullptr;
+    {
+      std::lock_guard<std::mutex> g(c.leo->mu);
+      tbl = c.leo->d_dense_enc;
+    }
+    const size_t total = c.k + c.m;
+    std::vector<JobDesc> jobs(n);
+    std::vector<const uint8_t *> ptrs(shards, shards + n * total);
+    for (size_t i = 0; i < n; ++i) {
+      jobs[i].ptr_off = uint32_t(i * total);
+      jobs[i].n_in = uint16_t(c.k);
+      jobs[i].n_out = uint16_t(c.m);
+      jobs[i].tbl = tbl;
+    }
+    return c.apply_jobs(jobs, ptrs, len, s);
+  }
   return run_once(c, RSGPU_OP_ENCODE, n, shards, nullptr, len, 0, nullptr, 0, nullptr, s);
 }
 
@@ -1129,7 +1160,7 @@ int leopard_dense_encode(Codec &c, std::vector<uint8_t> &rows) {
   if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, s));
   std::vector<uint8_t *> ptrs(total);
   for (size_t i = 0; i < total; ++i) ptrs[i] = d + i * L;
-  if (rc == RSGPU_OK) rc = leopard_encode(c, 1, ptrs.data(), L, s);
+  if (rc == RSGPU_OK) rc = run_once(c, RSGPU_OP_ENCODE, 1, ptrs.data(), nullptr, L, 0, nullptr, 0, nullptr, s);
   if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpyAsync(host.data(), d, host.size(), cudaMemcpyDeviceToHost, s));
   if (d) cudaFreeAsync(d, s);
   if (cudaStreamSynchronize(s) != cudaSuccess && rc == RSGPU_OK) rc = RSGPU_ERR_CUDA;
@@ -1138,8 +1169,18 @@ int leopard_dense_encode(Codec &c, std::vector<uint8_t> &rows) {
   rows.assign(m * k, 0);
   for (size_t r = 0; r < m; ++r)
     for (size_t j = 0; j < k; ++j) rows[r * k + j] = host[(k + r) * L + j];
+  std::vector<uint32_t> packed(packed_table_words(m, k));
+  pack_tables_with(leopard_mul8(), rows.data(), m, k, packed.data());
+  uint32_t *d_tbl = nullptr;
+  RS_CUDA(cudaMalloc(&d_tbl, packed.size() * 4));
+  RS_CUDA(cudaMemcpy(d_tbl, packed.data(), packed.size() * 4, cudaMemcpyHostToDevice));
   std::lock_guard<std::mutex> g(st.mu);
+  if (!st.dense_enc.empty()) {  // another thread finished first
+    cudaFree(d_tbl);
+    return RSGPU_OK;
+  }
   st.dense_enc = rows;
+  st.d_dense_enc = d_tbl;
   return RSGPU_OK;
 }
 

@@ -72,6 +72,25 @@ def test_leopard_encode_matches_oracle(rs, torch, field, k, m, size):
     assert not c.verify(bad)
 
 
+@pytest.mark.parametrize("k,m,size", [(10, 4, 262144), (4, 2, 131072), (1, 1, 131072), (7, 3, 131072 + 64)])
+def test_lgf8_dense_encode_matches_oracle(rs, torch, k, m, size):
+    # GF(2^8) codes with <= 4 parity shards encode shards >= 128 KiB through
+    # K1 with the dense encode map; verify still runs the FFT encode, so the
+    # two paths check each other too.
+    rng = np.random.default_rng(k * 100 + m)
+    data = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)]
+    rc, par = O.leopard_encode(8, k, m, data)
+    assert rc == 0
+    c = codec(rs, 8, k, m)
+    for _ in range(2):  # the second call reuses the cached device tables
+        sh = dev(torch, data + [np.full(size, 0x33, np.uint8) for _ in range(m)])
+        c.encode(sh)
+        out = host(sh)
+        for i in range(m):
+            assert np.array_equal(out[k + i], par[i]), (k, m, i)
+        assert c.verify(sh)
+
+
 @pytest.mark.parametrize("field,k,m,size", ENC_SHAPES)
 @pytest.mark.parametrize("codeword", [True, False])
 def test_leopard_reconstruct_matches_oracle(rs, torch, field, k, m, size, codeword):
