@@ -367,6 +367,9 @@ struct LeopardState {
   std::list<DenseEntry> dense_lru;
   std::unordered_map<std::string, std::list<DenseEntry>::iterator> dense_index;
   size_t dense_bytes = 0;
+  // Bytes reconstructed so far under patterns whose map is not derived yet
+  // (bounded: cleared when it holds kDenseSeenMax patterns).
+  std::unordered_map<std::string, size_t> dense_seen;
   ~LeopardState() {
     cudaDeviceSynchronize();
     for (void *p : plan_slabs) cudaFree(p);
@@ -976,7 +979,13 @@ int leopard_verify(Codec &c, size_t n, const uint8_t *const *shards, size_t len,
 namespace {
 
 constexpr size_t kDenseCacheBytes = size_t(64) << 20;
-constexpr size_t kDenseMinLen = size_t(32) << 10;  // below: only cached maps go dense
+// A pattern's map is derived once the calls of this codec have moved this
+// many bytes under it (this call included): deriving costs a small FFT
+// launch, a wait and host packing (about a millisecond), which the FFT decode
+// (~150 GB/s) of fewer bytes finishes sooner, while a pattern that keeps
+// coming back (a failed disk seen by every stripe) soon pays for it.
+constexpr size_t kDenseDeriveBytes = size_t(64) << 20;
+constexpr size_t kDenseSeenMax = 4096;
 constexpr size_t kDenseWideLen = size_t(1) << 20;  // maps of > 4 output groups: dense from here
 constexpr int kDenseNotTaken = -1;
 
@@ -986,56 +995,97 @@ constexpr int kDenseNotTaken = -1;
 // pipeline's own linear map, so the bytes are the FFT decode's on any
 // inputs; measured 2.8-6x faster than the per-call FFT decode on 32+16
 // codes (1-4 MiB shards) and on 128+64 with up to 16 erasures.
-// kDenseNotTaken (use the FFT decode) when the shards are short and some
-// pattern is not cached yet (a derivation costs a small launch and a wait,
-// more than the FFT decode of short shards), and when a map has more than 16
-// targets and the shards are under 1 MiB (its K1 tables and extra passes over
-// the inputs then cost more than the transform: 128+64 with 64 erasures at
-// 256 KiB took 7.2 ms dense against 3.9 ms FFT).
+// A pattern stays on the FFT decode while its map is not cached and fewer
+// than kDenseDeriveBytes have been moved under it, and when its map has more
+// than 16 targets and the shards are under 1 MiB (its K1 tables and extra
+// passes over the inputs then cost more than the transform: 128+64 with 64
+// erasures at 256 KiB took 7.2 ms dense against 3.9 ms FFT); those stripes
+// run in one FFT launch beside the dense one.  kDenseNotTaken when no
+// pattern goes dense.
 int reconstruct_dense8(Codec &c, size_t n, uint8_t *const *shards, const uint8_t *present, size_t len, int goal,
                        cudaStream_t s) {
   LeopardState &st = *c.leo;
   const size_t k = c.k, total = k + c.m;
+  // Distinct patterns of the stripes that have something to rebuild.
   std::unordered_map<std::string, size_t> uniq;
-  std::vector<size_t> which(n, SIZE_MAX);
-  std::vector<uint8_t> pres;
-  size_t max_targets = 0;
+  std::vector<size_t> which(n, SIZE_MAX), stripes_of, targets_of;
+  std::vector<std::string> keys;
   for (size_t i = 0; i < n; ++i) {
     const uint8_t *pr = present + i * total;
     size_t targets = 0;
     for (size_t x = 0; x < total; ++x) targets += !pr[x] && (goal == RSGPU_GOAL_ALL || x < k);
     if (!targets) continue;
-    max_targets = std::max(max_targets, targets);
     std::string key(reinterpret_cast<const char *>(pr), total);
     auto it = uniq.find(key);
     if (it == uniq.end()) {
-      it = uniq.emplace(key, uniq.size()).first;
-      pres.insert(pres.end(), key.begin(), key.end());
+      it = uniq.emplace(key, keys.size()).first;
+      keys.push_back(key);
+      stripes_of.push_back(0);
+      targets_of.push_back(targets);
     }
     which[i] = it->second;
+    ++stripes_of[it->second];
   }
-  if (uniq.empty()) return RSGPU_OK;
-  if (max_targets > 16 && len < kDenseWideLen) return kDenseNotTaken;
-  if (len < kDenseMinLen) {
+  if (keys.empty()) return RSGPU_OK;
+  // Which patterns run dense.
+  std::vector<char> dense(keys.size(), 1);
+  size_t n_dense = 0;
+  {
     std::lock_guard<std::mutex> g(st.mu);
-    for (auto &kv : uniq)
-      if (!st.dense_index.count(kv.first + char(goal))) return kDenseNotTaken;
+    for (size_t u = 0; u < keys.size(); ++u) {
+      const std::string key = keys[u] + char(goal);
+      if (targets_of[u] > 16 && len < kDenseWideLen) {
+        dense[u] = 0;
+      } else if (!st.dense_index.count(key)) {
+        if (st.dense_seen.size() >= kDenseSeenMax) st.dense_seen.clear();
+        size_t &seen = st.dense_seen[key];
+        seen += stripes_of[u] * total * len;
+        if (seen < kDenseDeriveBytes)
+          dense[u] = 0;
+        else
+          st.dense_seen.erase(key);
+      }
+      n_dense += dense[u];
+    }
   }
+  if (n_dense == 0) return kDenseNotTaken;
+  // The other patterns' stripes: one FFT decode launch on the same stream.
+  if (n_dense < keys.size()) {
+    std::vector<uint8_t *> fsh;
+    std::vector<uint8_t> fpr;
+    for (size_t i = 0; i < n; ++i) {
+      if (which[i] == SIZE_MAX || dense[which[i]]) continue;
+      fsh.insert(fsh.end(), shards + i * total, shards + (i + 1) * total);
+      fpr.insert(fpr.end(), present + i * total, present + (i + 1) * total);
+    }
+    const int rc = run_once(c, RSGPU_OP_RECONSTRUCT, fsh.size() / total, fsh.data(), fpr.data(), len, goal, nullptr,
+                            0, nullptr, s);
+    if (rc) return rc;
+  }
+  // Dense patterns: maps (cached or derived), then one K1 launch.
+  std::vector<size_t> slot(keys.size(), SIZE_MAX);
+  std::vector<uint8_t> pres;
+  for (size_t u = 0; u < keys.size(); ++u)
+    if (dense[u]) {
+      slot[u] = pres.size() / total;
+      pres.insert(pres.end(), keys[u].begin(), keys[u].end());
+    }
   std::vector<LeoDenseMap> maps;
-  int rc = leopard_dense_decode(c, uniq.size(), pres.data(), goal, maps, s);
+  int rc = leopard_dense_decode(c, n_dense, pres.data(), goal, maps, s);
   if (rc) return rc;
   std::vector<uint32_t> tables;
   std::vector<size_t> map_off(maps.size());
-  for (size_t u = 0; u < maps.size(); ++u) {
-    map_off[u] = tables.size();
-    tables.insert(tables.end(), maps[u].packed->begin(), maps[u].packed->end());
+  for (size_t d = 0; d < maps.size(); ++d) {
+    map_off[d] = tables.size();
+    tables.insert(tables.end(), maps[d].packed->begin(), maps[d].packed->end());
   }
   std::vector<JobDesc> jobs;
   std::vector<size_t> tbl_off;
   std::vector<const uint8_t *> ptrs;
   for (size_t i = 0; i < n; ++i) {
-    if (which[i] == SIZE_MAX) continue;
-    const LeoDenseMap &mp = maps[which[i]];
+    if (which[i] == SIZE_MAX || !dense[which[i]]) continue;
+    const size_t d = slot[which[i]];
+    const LeoDenseMap &mp = maps[d];
     JobDesc j{};
     j.ptr_off = uint32_t(ptrs.size());
     j.n_in = uint16_t(mp.inputs.size());
@@ -1043,7 +1093,7 @@ int reconstruct_dense8(Codec &c, size_t n, uint8_t *const *shards, const uint8_t
     for (uint16_t x : mp.inputs) ptrs.push_back(shards[i * total + x]);
     for (uint16_t t : mp.targets) ptrs.push_back(shards[i * total + t]);
     jobs.push_back(j);
-    tbl_off.push_back(map_off[which[i]]);
+    tbl_off.push_back(map_off[d]);
   }
   return c.apply_with_tables(jobs, tbl_off, ptrs, tables, len, s);
 }

@@ -210,16 +210,16 @@ def test_lgf16_wide_decode_matches_oracle(rs, torch, k, m, size, codeword):
             assert np.array_equal(lst[i].cpu().numpy(), ref[i]), (k, m, e, i)
 
 
-@pytest.mark.parametrize("k,m", [(4, 2), (32, 16), (128, 64)])
-def test_lgf8_dense_reconstruct_matches_oracle(rs, torch, k, m):
-    # GF(2^8) reconstructs of shards >= 32 KiB with <= 16 targets run the
-    # pattern's dense map through K1 (wider maps on short shards run the FFT
-    # decode); arbitrary (non-codeword) inputs pin both to the reference.
-    size = 65536 + 3 * 64  # Leopard shards are 64-byte multiples
+@pytest.mark.parametrize("k,m,size", [(4, 2, 12 << 20), (32, 16, 1536 << 10), (128, 64, 384 << 10)])
+def test_lgf8_dense_reconstruct_matches_oracle(rs, torch, k, m, size):
+    # GF(2^8) reconstructs that move >= 64 MiB under a pattern (here one
+    # ~72 MiB stripe) derive its dense map and run it through K1; the same
+    # pattern on short shards then hits the cached map.  Arbitrary
+    # (non-codeword) inputs pin the dense path to the reference's decode.
     rng = np.random.default_rng(k * 31 + m)
     full = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k + m)]
     c = codec(rs, 8, k, m)
-    for e, goal in ((m, "all"), (min(16, max(1, m // 3)), "all"), (min(16, m), "data")):
+    for e, goal in ((min(16, m), "all"), (max(1, m // 3), "all"), (min(16, m), "data")):
         lost = set(rng.choice(k + m, size=e, replace=False).tolist())
         pres = [0 if i in lost else 1 for i in range(k + m)]
         ref = [s.copy() for s in full]
@@ -234,7 +234,7 @@ def test_lgf8_dense_reconstruct_matches_oracle(rs, torch, k, m):
                 assert lst[i] is None
             else:
                 assert np.array_equal(lst[i].cpu().numpy(), ref[i]), (k, m, e, goal, i)
-        # The same pattern on short shards: a cached map also runs dense.
+        del buf, lst
         short = [s[:64].copy() for s in full]
         sref = [s[:64].copy() for s in ref]
         sbuf = torch.from_numpy(np.stack(short)).cuda()
@@ -245,19 +245,45 @@ def test_lgf8_dense_reconstruct_matches_oracle(rs, torch, k, m):
                 assert np.array_equal(slst[i].cpu().numpy(), sref[i]), (k, m, e, goal, i, "short")
 
 
-def test_lgf8_dense_batch_of_mixed_patterns(rs, torch):
-    # Several stripes, several patterns (one repeated, one stripe with nothing
-    # to do) in one host-memory batch call.
-    k, m, size, n = 32, 16, 40960, 6
+def test_lgf8_repeated_pattern_switches_to_dense(rs, torch):
+    # 48 MiB per call under one pattern: the first call runs the FFT decode,
+    # the second crosses the codec's 64 MiB tally and derives the dense map,
+    # the third uses the cached map; every call must give the same bytes.
+    k, m, size = 32, 16, 1 << 20
+    rng = np.random.default_rng(4242)
+    full = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k + m)]
+    lost = set(rng.choice(k + m, size=7, replace=False).tolist())
+    pres = [0 if i in lost else 1 for i in range(k + m)]
+    ref = [s.copy() for s in full]
+    for i in lost:
+        ref[i][:] = 0
+    assert O.leopard_reconstruct(8, k, m, ref, pres) == 0
+    c = codec(rs, 8, k, m)
+    for call in range(3):
+        buf = torch.from_numpy(np.stack(full)).cuda()
+        lst = [None if i in lost else buf[i] for i in range(k + m)]
+        c.reconstruct(lst)
+        for i in sorted(lost):
+            assert np.array_equal(lst[i].cpu().numpy(), ref[i]), (call, i)
+
+
+def test_lgf8_dense_and_fft_in_one_batch(rs, torch):
+    # One host-memory batch: 24 stripes under one pattern (72 MiB: dense),
+    # five stripes with patterns of their own (too few bytes: FFT decode, in
+    # a second launch), one stripe with nothing to rebuild.
+    k, m, size, n = 32, 16, 65536, 30
     rng = np.random.default_rng(77)
     c = codec(rs, 8, k, m)
+    shared = set(rng.choice(k + m, size=9, replace=False).tolist())
     stripes, pats, refs = [], [], []
     for s in range(n):
         full = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k + m)]
-        e = 0 if s == 3 else int(rng.integers(1, m + 1))
-        lost = set(rng.choice(k + m, size=e, replace=False).tolist()) if e else set()
-        if s == 5:
-            lost = {i for i, p in enumerate(pats[1]) if not p}  # repeats stripe 1's pattern
+        if s < 24:
+            lost = shared
+        elif s < 29:
+            lost = set(rng.choice(k + m, size=int(rng.integers(1, m + 1)), replace=False).tolist())
+        else:
+            lost = set()
         pres = [0 if i in lost else 1 for i in range(k + m)]
         ref = [x.copy() for x in full]
         for i in lost:
