@@ -427,11 +427,13 @@ int Codec::encode_dev(size_t n_stripes, uint8_t *const *shards, size_t len, cuda
   return run_apply(jobs, ptrs, len, false, nullptr, s);
 }
 
-int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok_host,
-                      cudaStream_t s) {
+int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok_host, cudaStream_t s,
+                      const uint32_t *tbl) {
   std::vector<JobDesc> jobs;
   std::vector<const uint8_t *> ptrs;
   encode_jobs(n_stripes, const_cast<uint8_t *const *>(shards), jobs, ptrs, true);
+  if (tbl)
+    for (auto &j : jobs) j.tbl = tbl;
   uint32_t *flags = nullptr;
   RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&flags), n_stripes * 4, s));
   RS_CUDA(cudaMemsetAsync(flags, 0, n_stripes * 4, s));

@@ -128,8 +128,10 @@ class Codec {
 
   // ---- operations; pointers are device pointers unless noted
   int encode_dev(size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s);
-  int verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok_host,
-                 cudaStream_t s);
+  // `tbl`: packed parity tables to check against (default: this codec's
+  // encode tables d_enc_tbl).
+  int verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len, uint8_t *ok_host, cudaStream_t s,
+                 const uint32_t *tbl = nullptr);
   // Verify without waiting: stripe i ORs 1 into flags_dev[i] on a mismatch.
   int verify_dev_async(size_t n_stripes, uint8_t *const *shards, size_t len, uint32_t *flags_dev, cudaStream_t s);
   int reconstruct_dev(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,

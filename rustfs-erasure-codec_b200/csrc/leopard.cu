@@ -963,6 +963,19 @@ int leopard_encode(Codec &c, size_t n, uint8_t *const *shards, size_t len, cudaS
 }
 
 int leopard_verify(Codec &c, size_t n, const uint8_t *const *shards, size_t len, uint8_t *ok, cudaStream_t s) {
+  // The same rule as encode: small-parity GF(2^8) codes on shards of 128 KiB
+  // and more compare against the dense encode map through K1.
+  if (c.leo->field->bits == 8 && c.m <= 4 && len >= kDenseEncMinLen && n > 0) {
+    std::vector<uint8_t> rows;
+    int rc = leopard_dense_encode(c, rows);
+    if (rc) return rc;
+    const uint32_t *tbl = nullptr;
+    {
+      std::lock_guard<std::mutex> g(c.leo->mu);
+      tbl = c.leo->d_dense_enc;
+    }
+    return c.verify_dev(n, shards, len, ok, s, tbl);
+  }
   uint32_t *flags = nullptr;
   RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&flags), std::max<size_t>(n, 1) * 4, s));
   RS_CUDA(cudaMemsetAsync(flags, 0, std::max<size_t>(n, 1) * 4, s));

@@ -74,9 +74,9 @@ def test_leopard_encode_matches_oracle(rs, torch, field, k, m, size):
 
 @pytest.mark.parametrize("k,m,size", [(10, 4, 262144), (4, 2, 131072), (1, 1, 131072), (7, 3, 131072 + 64)])
 def test_lgf8_dense_encode_matches_oracle(rs, torch, k, m, size):
-    # GF(2^8) codes with <= 4 parity shards encode shards >= 128 KiB through
-    # K1 with the dense encode map; verify still runs the FFT encode, so the
-    # two paths check each other too.
+    # GF(2^8) codes with <= 4 parity shards encode and verify shards >= 128 KiB
+    # through K1 with the dense encode map (the smaller shapes above run the
+    # FFT kernels, so the two forms are each checked against the oracle).
     rng = np.random.default_rng(k * 100 + m)
     data = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)]
     rc, par = O.leopard_encode(8, k, m, data)
@@ -89,6 +89,9 @@ def test_lgf8_dense_encode_matches_oracle(rs, torch, k, m, size):
         for i in range(m):
             assert np.array_equal(out[k + i], par[i]), (k, m, i)
         assert c.verify(sh)
+        bad = [t.clone() for t in sh]
+        bad[k + m - 1][size // 2] ^= 0x10
+        assert not c.verify(bad)
 
 
 @pytest.mark.parametrize("field,k,m,size", ENC_SHAPES)
