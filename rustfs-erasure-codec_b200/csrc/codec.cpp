@@ -347,7 +347,9 @@ int ApplyLaunch::build(std::vector<JobDesc> &jobs, const std::vector<const uint8
   max_tail = 0;
   uint32_t max_out = 0;
   int any_vec = 0;
+  int tbl_stage = 0;
   for (auto &j : jobs) {
+    tbl_stage |= j.tbl != jobs[0].tbl;
     bool aligned = true;
     for (uint32_t i = 0; i < uint32_t(j.n_in) + j.n_out; ++i)
       aligned &= (reinterpret_cast<uintptr_t>(ptrs[j.ptr_off + i]) & 15) == 0;
@@ -375,6 +377,7 @@ int ApplyLaunch::build(std::vector<JobDesc> &jobs, const std::vector<const uint8
   args.n_jobs = uint32_t(jobs.size());
   args.max_out = max_out;
   args.any_vec = any_vec;
+  args.tbl_stage = tbl_stage;
   args.accumulate = accumulate ? 1 : 0;
   return RSGPU_OK;
 }

@@ -88,6 +88,11 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
+__device__ __forceinline__ uint32_t lds32(uint32_t addr) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
 __device__ __forceinline__ uint4 lds128(uint32_t addr) {
   uint4 v;
   asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr)
@@ -100,8 +105,16 @@ __global__ void __launch_bounds__(kApplyThreads + 32, 2) k_apply_tma(ApplyArgs a
   constexpr uint32_t kSlot = kApplyThreads * kApplyVec * V;  // one input's slice of a tile
   extern __shared__ __align__(128) uint8_t tma_smem[];
   __shared__ __align__(8) uint64_t full[S], empty[S];
+  // The 4+4 nibble tables (words 0..31 of each input's packed table) of each
+  // stage's inputs, copied with the data when the launch's jobs carry
+  // different tables (a batch of stripes with different erasure patterns):
+  // read from L2 after the stage's wait, they put an L2 round trip on every
+  // step (10+4 rebuild 3.2 -> 4.2 TB/s).  A table that every job shares stays
+  // L1-resident and is read with plain loads.
+  __shared__ __align__(16) uint32_t tma_tbl[S][4][32];
   const uint32_t tid = threadIdx.x, lane = tid & 31;
   const uint32_t sbase = uint32_t(__cvta_generic_to_shared(tma_smem));
+  const uint32_t tbase = uint32_t(__cvta_generic_to_shared(&tma_tbl[0][0][0]));
   const uint32_t fbar = uint32_t(__cvta_generic_to_shared(full));
   const uint32_t ebar = uint32_t(__cvta_generic_to_shared(empty));
   if (tid == 0) {
@@ -126,6 +139,7 @@ __global__ void __launch_bounds__(kApplyThreads + 32, 2) k_apply_tma(ApplyArgs a
       if (base >= d.vec_len) continue;
       const uint32_t valid = uint32_t(d.vec_len - base < kSlot ? d.vec_len - base : kSlot);
       const uint8_t *const *ptr = a.ptrs + d.ptr_off;
+      const bool tbl_copy = a.tbl_stage && d.tbl && (reinterpret_cast<uintptr_t>(d.tbl) & 15) == 0;
       const uint32_t steps = (d.n_in + 3) / 4 + (VERIFY ? 1 : 0);
       for (uint32_t step = 0; step < steps; ++step, ++it) {
         const uint32_t s = it % S, ph = (it / S) & 1;
@@ -136,9 +150,13 @@ __global__ void __launch_bounds__(kApplyThreads + 32, 2) k_apply_tma(ApplyArgs a
         const bool par = VERIFY && step * 4 >= d.n_in;
         const uint32_t j0 = par ? d.n_in : step * 4;
         const uint32_t rows = par ? d.n_out : min(4u, d.n_in - j0);
-        mbar_expect_tx(fbar + 8 * s, rows * valid);
+        const bool tbl_here = tbl_copy && !par;
+        mbar_expect_tx(fbar + 8 * s, rows * valid + (tbl_here ? rows * 128 : 0));
         for (uint32_t b = 0; b < rows; ++b)
           bulk_load(sbase + (s * 4 + b) * kSlot, ptr[j0 + b] + base, valid, fbar + 8 * s);
+        if (tbl_here)
+          for (uint32_t b = 0; b < rows; ++b)
+            bulk_load(tbase + (s * 4 + b) * 128, d.tbl + (j0 + b) * kTableWords, 128, fbar + 8 * s);
       }
     }
     if (!ok) {
@@ -161,6 +179,7 @@ __global__ void __launch_bounds__(kApplyThreads + 32, 2) k_apply_tma(ApplyArgs a
     const JobDesc d = a.jobs[job];
     if (base >= d.vec_len) continue;
     const uint32_t n_in = d.n_in;
+    const bool tbl_copy = a.tbl_stage && d.tbl && (reinterpret_cast<uintptr_t>(d.tbl) & 15) == 0;  // as the producer decides
     const uint32_t steps = (n_in + 3) / 4 + (VERIFY ? 1 : 0);
     uint64_t col[V];
     bool active[V];
@@ -188,9 +207,16 @@ __global__ void __launch_bounds__(kApplyThreads + 32, 2) k_apply_tma(ApplyArgs a
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
           if (j0 + b >= n_in) break;  // warp-uniform
-          const uint32_t *tb = d.tbl + (j0 + b) * kTableWords;
-          const uint32_t lo = __ldg(tb + (lane & 15));
-          const uint32_t hi = __ldg(tb + 16 + (lane & 15));
+          uint32_t lo, hi;
+          if (tbl_copy) {
+            const uint32_t ta = tbase + (s * 4 + b) * 128 + (lane & 15) * 4;
+            lo = lds32(ta);
+            hi = lds32(ta + 64);
+          } else {
+            const uint32_t *tb = d.tbl + (j0 + b) * kTableWords;
+            lo = __ldg(tb + (lane & 15));
+            hi = __ldg(tb + 16 + (lane & 15));
+          }
 #pragma unroll
           for (int v = 0; v < V; ++v) {
             const uint4 x = lds128(slot0 + b * kSlot + v * kApplyThreads * kApplyVec);

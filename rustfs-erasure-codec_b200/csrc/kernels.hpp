@@ -18,6 +18,7 @@ struct ApplyArgs {
   int any_vec;                  // some job has vec_len > 0
   int accumulate;               // outputs ^= products (incremental parity update)
   uint32_t *stall;              // device status word: a bounded wait of the TMA-staged tile ran out (may be null)
+  int tbl_stage;                // jobs carry different tables: the TMA-staged tile copies them with the data
 };
 cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cudaStream_t s);
 // K1 tile for launches of at most 4 outputs: 0 (default) TMA-staged, 1 the
