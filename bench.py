@@ -879,7 +879,9 @@ def e2e_measure(torch, rsgpu, args, group):
         eb, rb, vb = step_bytes(k, m, pats, SHARD)
         total += eb + rb + vb
         e = (k + m) - pats.sum(axis=1)
-        h2d += n * k * SHARD + int(((k + m - e) * SHARD).sum()) + n * (k + m) * SHARD
+        # encode uploads the data shards, rebuild the first k present shards
+        # (the survivors a classic decode reads), verify every shard.
+        h2d += n * k * SHARD + n * k * SHARD + n * (k + m) * SHARD
         d2h += n * m * SHARD + int((e * SHARD).sum()) + n
         stripes.append((codec, lists, pats, host))
 
@@ -907,9 +909,10 @@ def e2e_measure(torch, rsgpu, args, group):
     for codec, lists, pats, host in stripes:
         del host
     link = host_link_gbs(torch)
-    # The link's own bound for this step: the two directions use separate copy
-    # engines, so the larger of the two transfer times.
-    bound = max(h2d / (link["h2d_gbs"] * 1e9), d2h / (link["d2h_gbs"] * 1e9))
+    # The link's own bound for this step: each direction alone, and both
+    # together at the rate the link sustains with copies in flight both ways.
+    bound = max(h2d / (link["h2d_gbs"] * 1e9), d2h / (link["d2h_gbs"] * 1e9),
+                (h2d + d2h) / (link["both_gbs"] * 1e9))
     total *= group.ranks.world
     h2d *= group.ranks.world
     d2h *= group.ranks.world
@@ -921,8 +924,9 @@ def e2e_measure(torch, rsgpu, args, group):
 
 
 def host_link_gbs(torch, nbytes=2 << 30, reps=5):
-    """Pinned host <-> device copy bandwidth of this GPU (one 2 GiB copy each
-    way, best of reps, CUDA events): the ceiling of the host-memory path."""
+    """Pinned host <-> device copy bandwidth of this GPU (a 2 GiB copy each
+    way alone, and one each way at once; best of reps, CUDA events): the
+    ceiling of the host-memory path."""
     h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
     d = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     out = {}
@@ -938,7 +942,30 @@ def host_link_gbs(torch, nbytes=2 << 30, reps=5):
             t = e0.elapsed_time(e1) / 1e3
             best = t if best is None else min(best, t)
         out[name] = round(nbytes / best / 1e9, 1)
-    del h, d
+    # Both directions at once on two streams (a second pair of buffers):
+    # bytes moved both ways over the time until both copies finished.
+    h2 = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d2 = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s_up, s_down = torch.cuda.Stream(), torch.cuda.Stream()
+    best = None
+    for _ in range(reps):
+        cur = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        s_up.wait_stream(cur)
+        s_down.wait_stream(cur)
+        with torch.cuda.stream(s_up):
+            d.copy_(h, non_blocking=True)
+        with torch.cuda.stream(s_down):
+            h2.copy_(d2, non_blocking=True)
+        cur.wait_stream(s_up)
+        cur.wait_stream(s_down)
+        e1.record(cur)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        best = t if best is None else min(best, t)
+    out["both_gbs"] = round(2 * nbytes / best / 1e9, 1)
+    del h, d, h2, d2
     return out
 
 

@@ -228,6 +228,17 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
   RS_CUDA(cudaEventRecord(ev, S(user_stream)));
   RS_CUDA(cudaStreamWaitEvent(h->io[0], ev, 0));
   RS_CUDA(cudaStreamWaitEvent(h->io[1], ev, 0));
+  // A classic GF(2^8) verify writes the mismatch flags of the whole call into
+  // one device array that is read back once at the end, so no chunk waits
+  // on the host for its own result before the next chunk's copies are queued.
+  // The other families report per chunk.
+  uint32_t *vflags = nullptr;
+  if (op == OP_VERIFY && c.family == RSGPU_FAMILY_CLASSIC && c.field == RSGPU_FIELD_GF8) {
+    RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&vflags), std::max<size_t>(n_stripes, 1) * 4, h->io[0]));
+    RS_CUDA(cudaMemsetAsync(vflags, 0, std::max<size_t>(n_stripes, 1) * 4, h->io[0]));
+    RS_CUDA(cudaEventRecord(ev, h->io[0]));
+    RS_CUDA(cudaStreamWaitEvent(h->io[1], ev, 0));
+  }
   cudaEventDestroy(ev);
   const size_t pitch = round16(len);
   const size_t per = chunk_stripes(total * pitch);
@@ -246,11 +257,17 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
     for (size_t i = 0; i < cnt * total; ++i) dptr[i] = stage + i * pitch;
     // Inputs are queued first; the job-table upload and the kernel follow them
     // on the same stream.
+    // A classic rebuild reads only the first k present shards (the plan's
+    // survivors, src/core/recovery_plan.rs:329-387); Leopard reads every
+    // present shard.
     CopyRun up{cudaMemcpyHostToDevice, s};
+    const bool first_k = c.family == RSGPU_FAMILY_CLASSIC;
     for (size_t sidx = 0; sidx < cnt; ++sidx) {
       const size_t st = base + sidx;
+      size_t used = 0;
       for (size_t i = 0; i < total; ++i) {
         bool in = op == OP_ENCODE ? i < c.k : op == OP_VERIFY ? true : present[st * total + i] != 0;
+        if (op == OP_RECONSTRUCT && in) in = !first_k || used++ < c.k;
         if (in && (rc = up.add(dptr[sidx * total + i], host[st * total + i], len))) return rc;
       }
     }
@@ -258,7 +275,8 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
     if (op == OP_ENCODE)
       status = do_encode(c, cnt, dptr.data(), len, s);
     else if (op == OP_VERIFY)
-      status = do_verify(c, cnt, const_cast<const uint8_t *const *>(dptr.data()), len, ok + base, s);
+      status = vflags ? c.verify_dev_async(cnt, dptr.data(), len, vflags + base, s)
+                      : do_verify(c, cnt, const_cast<const uint8_t *const *>(dptr.data()), len, ok + base, s);
     else
       status = do_reconstruct(c, cnt, dptr.data(), present + base * total, len, goal, req, nreq, s);
     if (status == RSGPU_OK && op != OP_VERIFY) {
@@ -284,6 +302,15 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
   }
   RS_CUDA(cudaStreamSynchronize(h->io[0]));
   RS_CUDA(cudaStreamSynchronize(h->io[1]));
+  if (vflags) {
+    if (status == RSGPU_OK) {
+      std::vector<uint32_t> f(n_stripes);
+      RS_CUDA(cudaMemcpyAsync(f.data(), vflags, n_stripes * 4, cudaMemcpyDeviceToHost, h->io[0]));
+      RS_CUDA(cudaStreamSynchronize(h->io[0]));
+      for (size_t i = 0; i < n_stripes; ++i) ok[i] = f[i] ? 0 : 1;
+    }
+    RS_CUDA(cudaFreeAsync(vflags, h->io[0]));
+  }
   if (status == RSGPU_OK) status = c.take_device_status(h->io[0]);
   return status;
 }

@@ -328,6 +328,44 @@ def _buffer_info(shards):
     return mem, ptrs, lens, stream, keep
 
 
+def _stripe_block(stripes):
+    """(mem, ptr array, shard length, stream, keepalive) when `stripes` is one
+    C-contiguous (stripes, shards, length) uint8 block -- a numpy array or a
+    CUDA tensor -- with the pointers computed in one vectorised step; None for
+    any other form (lists of shards take the per-shard path)."""
+    if isinstance(stripes, np.ndarray):
+        if stripes.ndim != 3 or stripes.dtype != np.uint8 or not stripes.flags.c_contiguous:
+            return None
+        mem, stream, base = MEM_HOST, None, stripes.__array_interface__["data"][0]
+    elif _is_torch_cuda(stripes):
+        import torch
+
+        if stripes.dim() != 3 or stripes.dtype != torch.uint8 or not stripes.is_contiguous():
+            return None
+        mem, stream, base = MEM_DEVICE, torch.cuda.current_stream().cuda_stream, stripes.data_ptr()
+    else:
+        return None
+    n, t, length = stripes.shape
+    ptrs = np.uint64(base) + np.arange(max(1, n * t), dtype=np.uint64) * np.uint64(length)
+    return mem, ptrs.ctypes.data_as(PP), int(length), stream, (stripes, ptrs)
+
+
+def _check_stripe_widths(widths, total):
+    """Every stripe holds exactly k + m shards (TooFewShards / TooManyShards
+    otherwise, as the reference's per-call piece-count check)."""
+    for w in widths:
+        if w != total:
+            raise RsError(1 if w < total else 2)
+
+
+def _present_flags(present, n_stripes, n_shards):
+    """Presence flags as a uint8 array of n_stripes * n_shards entries."""
+    a = np.ascontiguousarray(np.asarray(present, dtype=bool), dtype=np.uint8).reshape(-1)
+    if a.size != n_stripes * n_shards:
+        raise ValueError("present must hold one flag per shard of every stripe")
+    return a, a.ctypes.data_as(U8P)
+
+
 def _flags(v, n):
     arr = (ctypes.c_uint8 * n)()
     for i, b in enumerate(v):
@@ -950,11 +988,29 @@ class ReedSolomon:
 
     # ---------------------------------------------------------- batched
     def encode_batch(self, stripes: Sequence[Sequence]) -> None:
+        """Encode every stripe.  `stripes` is a list of shard lists, or one
+        contiguous (stripes, k + m, length) uint8 array / CUDA tensor."""
+        blk = _stripe_block(stripes)
+        if blk is not None:
+            mem, ptrs, length, stream, keep = blk
+            _check_stripe_widths([stripes.shape[1]], self.total_shard_count())
+            _check(_lib().rsgpu_encode_batch(self._h, len(stripes), ptrs, length, mem, stream))
+            return
+        _check_stripe_widths([len(st) for st in stripes], self.total_shard_count())
         flat = [s for st in stripes for s in st]
         mem, ptrs, lens, stream, keep = _buffer_info(flat)
         _check(_lib().rsgpu_encode_batch(self._h, len(stripes), ptrs, lens[0] if flat else 0, mem, stream))
 
     def reconstruct_batch(self, stripes: Sequence[Sequence], present: Sequence[Sequence[bool]], goal="all") -> None:
+        blk = _stripe_block(stripes)
+        if blk is not None:
+            mem, ptrs, length, stream, keep = blk
+            _check_stripe_widths([stripes.shape[1]], self.total_shard_count())
+            n = len(stripes)
+            flags, pres = _present_flags(present, n, self.total_shard_count())
+            _check(_lib().rsgpu_reconstruct_batch(self._h, n, ptrs, pres, length, GOAL[goal], mem, stream))
+            return
+        _check_stripe_widths([len(st) for st in stripes], self.total_shard_count())
         flat = [s for st in stripes for s in st]
         mem, ptrs, lens, stream, keep = _buffer_info(flat)
         pres = _flags([p for row in present for p in row], len(flat))
@@ -966,6 +1022,15 @@ class ReedSolomon:
         return PreparedBatch(self, op, ptr_table, shard_len, present, goal)
 
     def verify_batch(self, stripes: Sequence[Sequence]) -> List[bool]:
+        blk = _stripe_block(stripes)
+        if blk is not None:
+            mem, ptrs, length, stream, keep = blk
+            _check_stripe_widths([stripes.shape[1]], self.total_shard_count())
+            n = len(stripes)
+            ok = np.zeros(max(1, n), dtype=np.uint8)
+            _check(_lib().rsgpu_verify_batch(self._h, n, ptrs, length, ok.ctypes.data_as(U8P), mem, stream))
+            return [bool(v) for v in ok[:n]]
+        _check_stripe_widths([len(st) for st in stripes], self.total_shard_count())
         flat = [s for st in stripes for s in st]
         mem, ptrs, lens, stream, keep = _buffer_info(flat)
         ok = (ctypes.c_uint8 * max(1, len(stripes)))()

@@ -265,6 +265,50 @@ def test_batch_host_path(rs):
     assert all(codec.verify_batch(stripes))
 
 
+@pytest.mark.parametrize("where", ["host", "device"])
+@pytest.mark.parametrize("size", [4096, 3000])
+def test_batch_stripe_block(rs, torch, where, size):
+    # One contiguous (stripes, k + m, length) block: pointers are computed in
+    # one step, a host rebuild uploads only the first k present shards, and a
+    # host verify reads back every chunk's flags once at the end.
+    k, m, n = 10, 4, 40
+    rng = np.random.default_rng(size + len(where))
+    codec = rs.ReedSolomon(k, m)
+    rc, mat = O.build_matrix(k, m)
+    ref = np.zeros((n, k + m, size), np.uint8)
+    ref[:, :k] = rng.integers(0, 256, (n, k, size), dtype=np.uint8)
+    for s in range(n):
+        st = list(ref[s])
+        O.classic_encode(mat, st)
+    blk = ref.copy()
+    blk[:, k:] = 0
+    if where == "device":
+        blk = torch.from_numpy(blk).cuda()
+    codec.encode_batch(blk)
+    got = blk if where == "host" else blk.cpu().numpy()
+    assert (got == ref).all()
+    pats = np.array(erase_patterns(rng, k, m, n), dtype=bool)
+    if where == "host":
+        blk[~pats] = 0xCC
+    else:
+        blk[torch.from_numpy(~pats).cuda()] = 0xCC
+    codec.reconstruct_batch(blk, pats)
+    got = blk if where == "host" else blk.cpu().numpy()
+    assert (got == ref).all()
+    assert codec.verify_batch(blk) == [True] * n
+    bad = [3, 17, n - 1]
+    for s in bad:
+        blk[s, k + s % m, size // 3] ^= 0x21
+    ok = codec.verify_batch(blk)
+    assert [i for i, v in enumerate(ok) if not v] == bad
+    with pytest.raises(rs.RsError) as e:
+        codec.verify_batch(blk[:, : k + m - 1])
+    assert e.value.name == "TooFewShards"
+    with pytest.raises(rs.RsError) as e:
+        codec.encode_batch([list(ref[0]) + [ref[0][0]]])
+    assert e.value.name == "TooManyShards"
+
+
 def test_error_precedence(rs, torch):
     codec = rs.ReedSolomon(4, 2)
     sh = [torch.zeros(64, dtype=torch.uint8, device="cuda") for _ in range(6)]
