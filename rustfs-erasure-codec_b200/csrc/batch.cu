@@ -395,6 +395,20 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   if (!forced) {
     int rc = mix_plan_batch(ops, n_ops, opt.planner, b.plans);
     if (rc) return rc;
+    // A one-shot batch (the request server's) runs a Leopard GF(2^8)
+    // rebuild through its dense map only when the per-call rule says so:
+    // the plan table prices launches, and deriving a new pattern's map (a
+    // small FFT launch, a wait and host packing) is host time that a batch
+    // run once cannot amortise.  Prepared batches keep the planner's choice.
+    if (b.stream_ordered)
+      for (size_t i = 0; i < n_ops; ++i) {
+        Codec &c = const_cast<rsgpu_codec *>(ops[i].codec)->c;
+        if (ops[i].op != RSGPU_OP_RECONSTRUCT || c.family != RSGPU_FAMILY_LEOPARD_GF8 ||
+            b.plans[i].algo != RSGPU_ALGO_APPLY)
+          continue;
+        if (!leopard_dense_due(c, ops[i].present, ops[i].goal, ops[i].shard_len))
+          b.plans[i] = mix_default_plan(c, ops[i].op, ops[i].shard_len);
+      }
   }
   for (size_t i = 0; i < n_ops; ++i) {
     Codec &c = const_cast<rsgpu_codec *>(ops[i].codec)->c;

@@ -1002,6 +1002,20 @@ constexpr size_t kDenseSeenMax = 4096;
 constexpr size_t kDenseWideLen = size_t(1) << 20;  // maps of > 4 output groups: dense from here
 constexpr int kDenseNotTaken = -1;
 
+// Whether a pattern (key = presence flags + goal) with `targets` outputs runs
+// through its dense map now, counting `bytes` more moved under it.  Caller
+// holds st.mu.
+bool dense_due_locked(LeopardState &st, const std::string &key, size_t targets, size_t bytes, size_t len) {
+  if (targets > 16 && len < kDenseWideLen) return false;
+  if (st.dense_index.count(key)) return true;
+  if (st.dense_seen.size() >= kDenseSeenMax) st.dense_seen.clear();
+  size_t &seen = st.dense_seen[key];
+  seen += bytes;
+  if (seen < kDenseDeriveBytes) return false;
+  st.dense_seen.erase(key);
+  return true;
+}
+
 // GF(2^8) reconstruct as a dense K1 launch: each stripe's map (its present
 // shards -> its targets) comes from the per-codec map cache, derived with
 // the FFT decode where missing (leopard_dense_decode).  The map is the FFT
@@ -1046,18 +1060,7 @@ int reconstruct_dense8(Codec &c, size_t n, uint8_t *const *shards, const uint8_t
   {
     std::lock_guard<std::mutex> g(st.mu);
     for (size_t u = 0; u < keys.size(); ++u) {
-      const std::string key = keys[u] + char(goal);
-      if (targets_of[u] > 16 && len < kDenseWideLen) {
-        dense[u] = 0;
-      } else if (!st.dense_index.count(key)) {
-        if (st.dense_seen.size() >= kDenseSeenMax) st.dense_seen.clear();
-        size_t &seen = st.dense_seen[key];
-        seen += stripes_of[u] * total * len;
-        if (seen < kDenseDeriveBytes)
-          dense[u] = 0;
-        else
-          st.dense_seen.erase(key);
-      }
+      dense[u] = dense_due_locked(st, keys[u] + char(goal), targets_of[u], stripes_of[u] * total * len, len);
       n_dense += dense[u];
     }
   }
@@ -1112,6 +1115,18 @@ int reconstruct_dense8(Codec &c, size_t n, uint8_t *const *shards, const uint8_t
 }
 
 }  // namespace
+
+bool leopard_dense_due(Codec &c, const uint8_t *present, int goal, size_t len) {
+  if (c.leo->field->bits != 8) return false;
+  const size_t k = c.k, total = k + c.m;
+  size_t targets = 0;
+  for (size_t x = 0; x < total; ++x) targets += !present[x] && (goal == RSGPU_GOAL_ALL || x < k);
+  if (!targets) return false;
+  const std::string key = std::string(reinterpret_cast<const char *>(present), total) + char(goal);
+  LeopardState &st = *c.leo;
+  std::lock_guard<std::mutex> g(st.mu);
+  return dense_due_locked(st, key, targets, total * len, len);
+}
 
 int leopard_reconstruct(Codec &c, size_t n, uint8_t *const *shards, const uint8_t *present, size_t len, int goal,
                         const uint8_t *required, size_t n_required, cudaStream_t s) {

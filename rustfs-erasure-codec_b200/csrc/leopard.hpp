@@ -71,6 +71,12 @@ struct LeoDenseMap {
 };
 int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, std::vector<LeoDenseMap> &maps,
                          cudaStream_t s);
+// Whether one GF(2^8) reconstruct (goal all or data) of this pattern should
+// run through the dense map now: its map is cached, or the codec's calls
+// have moved 64 MiB under the pattern, this one included (the per-call rule;
+// maps of more than 16 targets on shards under 1 MiB stay on the FFT decode).
+// Counts this call's bytes towards the pattern's tally.
+bool leopard_dense_due(Codec &c, const uint8_t *present, int goal, size_t len);
 
 int tower_encode(Codec &c, size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s);
 // Tower-field incremental parity: parity_r (+)= sum_j t[k + r][cols[j]] * inputs[j] (one stripe).
