@@ -337,6 +337,10 @@ __global__ void __launch_bounds__(1024) k_leo_locator(const uint8_t *const *pres
 struct LeoPlan {
   uint16_t *err = nullptr;  // device, n entries
   uint32_t input_count = 0;
+  // Completion of the launch that builds err (null once seen complete):
+  // a launch that uses the plan waits on it in stream order instead of the
+  // builder waiting on the host.
+  std::shared_ptr<CUevent_st> ready;
 };
 
 struct LeopardState {
@@ -688,10 +692,33 @@ int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>
   cudaFreeAsync(d_pres, s);
   cudaFreeAsync(d_pp, s);
   cudaFreeAsync(d_oo, s);
-  // The new plans are visible to other streams once the lock is released,
-  // so their locators must be complete: wait for this stream only.
-  RS_CUDA(cudaStreamSynchronize(s));
+  // The new plans are visible to other streams once the lock is released:
+  // their users wait for this event (wait_plans) rather than this thread
+  // waiting here, where the locator launch may queue behind other streams'
+  // long-running kernels.
+  cudaEvent_t ev = nullptr;
+  RS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  std::shared_ptr<CUevent_st> ready(ev, [](cudaEvent_t e) { cudaEventDestroy(e); });
+  RS_CUDA(cudaEventRecord(ev, s));
+  for (auto &p : pending) st.plans[p.first].ready = ready;
   pending.clear();
+  return RSGPU_OK;
+}
+
+// Makes stream s wait for the locator launches of these plans that may still
+// be running, and forgets the ones that have finished.  Caller holds st.mu.
+int wait_plans(const std::vector<LeoPlan *> &plans, cudaStream_t s) {
+  const CUevent_st *last = nullptr;
+  for (LeoPlan *p : plans) {
+    if (!p || !p->ready) continue;
+    if (cudaEventQuery(p->ready.get()) == cudaSuccess) {
+      p->ready.reset();
+      continue;
+    }
+    if (p->ready.get() == last) continue;
+    last = p->ready.get();
+    RS_CUDA(cudaStreamWaitEvent(s, p->ready.get(), 0));
+  }
   return RSGPU_OK;
 }
 
@@ -709,7 +736,9 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
   {
     std::lock_guard<std::mutex> g(st.mu);
     std::vector<std::pair<std::string, const uint8_t *>> pending;
-    for (size_t i = 0; i < n_stripes; ++i) {
+    std::vector<LeoPlan *> used;
+    int bad = RSGPU_OK;  // an unrecoverable stripe: plans already cached still get their locators
+    for (size_t i = 0; i < n_stripes && bad == RSGPU_OK; ++i) {
       LeoJob j{};
       j.ptr_off = uint32_t(i * total);
       j.flag_idx = uint32_t(i);
@@ -728,22 +757,27 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
         }
         // Missing beyond the parity count cannot be recovered
         // (src/core/leopard_gf16/decode.rs:744-748).
-        if (total - np > c.m) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+        if (total - np > c.m) {
+          bad = RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+          break;
+        }
         if (np == total || !any_target) {
           roles.resize(base);
           continue;
         }
         LeoPlan *plan = nullptr;
-        int rc = decode_plan(c, pr, &plan, s, pending);
-        if (rc) return rc;
+        if ((bad = decode_plan(c, pr, &plan, s, pending))) break;
         j.err = plan->err;
         j.input_count = plan->input_count;
+        used.push_back(plan);
         role_off.push_back(base);
       }
       jobs.push_back(j);
     }
     int rc = build_locators(c, pending, s);
+    if (!rc) rc = wait_plans(used, s);
     if (rc) return rc;
+    if (bad) return bad;
   }
   // Blob: jobs | pointers | roles.
   const size_t jb = jobs.size() * sizeof(LeoJob);
@@ -1173,12 +1207,12 @@ int leopard_locators(Codec &c, size_t n, const uint8_t *present, const uint16_t 
   const size_t total = c.k + c.m;
   std::lock_guard<std::mutex> g(st.mu);
   std::vector<std::pair<std::string, const uint8_t *>> pending;
-  std::vector<LeoPlan *> plans(n);
-  for (size_t i = 0; i < n; ++i) {
-    int rc = decode_plan(c, present + i * total, &plans[i], s, pending);
-    if (rc) return rc;
-  }
-  int rc = build_locators(c, pending, s);
+  std::vector<LeoPlan *> plans(n, nullptr);
+  int bad = RSGPU_OK;
+  for (size_t i = 0; i < n && bad == RSGPU_OK; ++i) bad = decode_plan(c, present + i * total, &plans[i], s, pending);
+  int rc = build_locators(c, pending, s);  // plans already cached get their locators even on an error
+  if (!rc) rc = wait_plans(plans, s);
+  if (!rc) rc = bad;
   if (rc) return rc;
   // unordered_map nodes are stable, so the plan pointers are still valid.
   for (size_t i = 0; i < n; ++i) {

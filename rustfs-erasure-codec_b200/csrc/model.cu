@@ -17,6 +17,8 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "batch.hpp"
@@ -203,6 +205,11 @@ struct ModelState {
   float *h_x = nullptr, *h_y = nullptr;
   size_t cap = 0;
   bool w_dirty = true;
+  // Predictions of this weight set by feature vector: a request stream
+  // repeats a few operation shapes, and a planner call whose shapes were all
+  // seen before launches nothing (its wait would queue behind whatever else
+  // occupies the device).  Cleared when the weights change.
+  std::unordered_map<std::string, std::vector<float>> memo;
 };
 ModelState &state() {
   static ModelState s;
@@ -253,6 +260,7 @@ int model_set(const float *in, size_t n) {
   state().params.assign(in, in + kParams);
   state().ready = true;
   state().w_dirty = true;
+  state().memo.clear();
   return RSGPU_OK;
 }
 
@@ -261,6 +269,19 @@ int model_predict(const float *features, size_t n, float *out) {
   std::lock_guard<std::mutex> g(m.mu);
   if (!m.ready) return RSGPU_ERR_INVALID_ARGUMENT;
   if (n == 0) return RSGPU_OK;
+  // Rows seen before come from the memo; the rest go to the device.
+  std::vector<size_t> miss;
+  for (size_t i = 0; i < n; ++i) {
+    auto it = m.memo.find(std::string(reinterpret_cast<const char *>(features + i * F), F * 4));
+    if (it == m.memo.end())
+      miss.push_back(i);
+    else
+      std::memcpy(out + i * P, it->second.data(), P * 4);
+  }
+  if (miss.empty()) return RSGPU_OK;
+  const float *all = features;
+  float *all_out = out;
+  n = miss.size();
   int dev = 0;
   RS_CUDA(cudaGetDevice(&dev));
   if (m.device != dev) {  // first use (or a new device): fresh context
@@ -287,7 +308,7 @@ int model_predict(const float *features, size_t n, float *out) {
     RS_CUDA(cudaStreamSynchronize(m.stream));
     m.w_dirty = false;
   }
-  std::memcpy(m.h_x, features, n * F * 4);
+  for (size_t x = 0; x < n; ++x) std::memcpy(m.h_x + x * F, all + miss[x] * F, F * 4);
   RS_CUDA(cudaMemcpyAsync(m.d_x, m.h_x, n * F * 4, cudaMemcpyHostToDevice, m.stream));
   k_mlp_sample<<<int(n), 32, 0, m.stream>>>(m.d_w, m.d_x, nullptr, nullptr, 0.f, int(n), m.d_y, nullptr, nullptr,
                                             nullptr, nullptr, nullptr, nullptr);
@@ -295,7 +316,12 @@ int model_predict(const float *features, size_t n, float *out) {
   RS_CUDA(cudaGetLastError());
   RS_CUDA(cudaMemcpyAsync(m.h_y, m.d_y, n * P * 4, cudaMemcpyDeviceToHost, m.stream));
   RS_CUDA(cudaStreamSynchronize(m.stream));
-  std::memcpy(out, m.h_y, n * P * 4);
+  if (m.memo.size() + n > 65536) m.memo.clear();
+  for (size_t x = 0; x < n; ++x) {
+    std::memcpy(all_out + miss[x] * P, m.h_y + x * P, P * 4);
+    m.memo.emplace(std::string(reinterpret_cast<const char *>(all + miss[x] * F), F * 4),
+                   std::vector<float>(m.h_y + x * P, m.h_y + (x + 1) * P));
+  }
   return RSGPU_OK;
 }
 
