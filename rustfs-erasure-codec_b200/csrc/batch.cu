@@ -40,6 +40,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <numeric>
 #include <string>
@@ -50,6 +51,7 @@
 #include "batch.hpp"
 #include "codec.hpp"
 #include "handles.hpp"
+#include "launch_cfg.hpp"
 #include "leo_fft.cuh"
 #include "leopard.hpp"
 
@@ -183,6 +185,18 @@ int sm_count() {
 }
 
 bool is_leopard(const Codec &c) { return c.family != RSGPU_FAMILY_CLASSIC; }
+
+// Resident k_mix CTAs per SM for a dynamic shared-memory size (the limit is
+// raised to the largest size a batch can ask for the first time it is
+// needed).
+cudaError_t mix_shape(size_t smem, int *per_sm) {
+  const void *fn = reinterpret_cast<const void *>(k_mix);
+  if (smem > 48 * 1024 - 1024) {
+    cudaError_t e = ensure_smem_limit(fn, std::max(smem, kMixSmem + (8 << 10)));
+    if (e != cudaSuccess) return e;
+  }
+  return blocks_per_sm(fn, kMixThreads, smem, per_sm);
+}
 bool is_tower(const Codec &c) { return c.family == RSGPU_FAMILY_CLASSIC && c.field != RSGPU_FIELD_GF8; }
 
 // Transform lanes of one column (m for encode / verify, n for decode); at
@@ -241,6 +255,7 @@ struct MixBatch {
   uint32_t *d_flags = nullptr;
   uint32_t *d_counter = nullptr;
   uint32_t *d_scratch = nullptr;
+  bool scratch_borrowed = false;  // d_scratch belongs to the caller's ScratchSlot
   MixArgs args{};
   size_t smem = 0;
   int grid = 0;
@@ -259,8 +274,9 @@ struct MixBatch {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (stream_ordered) {
-      for (void *p : {(void *)d_blob, (void *)d_flags, (void *)d_counter, (void *)d_scratch})
+      for (void *p : {(void *)d_blob, (void *)d_flags, (void *)d_counter})
         if (p) cudaFreeAsync(p, stream);
+      if (d_scratch && !scratch_borrowed) cudaFreeAsync(d_scratch, stream);
       return;
     }
     if (d_blob || d_flags || d_counter || d_scratch) cudaDeviceSynchronize();
@@ -372,7 +388,7 @@ int add_apply_job(MixBuild &B, const rsgpu_plan &plan, bool verify, size_t n_in,
 }  // namespace
 
 int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, const rsgpu_mix_options &opt,
-              MixPtr &out, cudaStream_t ordered) {
+              MixPtr &out, cudaStream_t ordered, ScratchSlot *scratch) {
   int device = 0;
   RS_CUDA(cudaGetDevice(&device));
   for (size_t i = 0; i < n_ops; ++i) {
@@ -730,14 +746,28 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
 
   // ---- launch shape
   b.smem = B.smem;
-  if (b.smem > 48 * 1024 - 1024)
-    RS_CUDA(cudaFuncSetAttribute(k_mix, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b.smem)));
   int per_sm = 0;
-  RS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mix, kMixThreads, b.smem));
+  RS_CUDA(mix_shape(b.smem, &per_sm));
   per_sm = std::max(per_sm, 1);
   if (opt.ctas_per_sm > 0) per_sm = std::min(per_sm, int(opt.ctas_per_sm));
   b.grid = int(std::max<uint64_t>(1, std::min<uint64_t>(items.size(), uint64_t(per_sm) * sm_count())));
-  if (B.scratch_words) RS_CUDA(b.alloc(&b.d_scratch, size_t(b.grid) * B.scratch_words * 4));
+  if (B.scratch_words) {
+    const size_t need = size_t(b.grid) * B.scratch_words * 4;
+    if (scratch && b.stream_ordered) {
+      if (scratch->bytes < need) {  // grow with headroom, in the stream's order
+        if (scratch->ptr) RS_CUDA(cudaFreeAsync(scratch->ptr, b.stream));
+        scratch->ptr = nullptr;
+        scratch->bytes = 0;
+        const size_t want = need + need / 4;
+        RS_CUDA(cudaMallocAsync(&scratch->ptr, want, b.stream));
+        scratch->bytes = want;
+      }
+      b.d_scratch = static_cast<uint32_t *>(scratch->ptr);
+      b.scratch_borrowed = true;
+    } else {
+      RS_CUDA(b.alloc(&b.d_scratch, need));
+    }
+  }
   MixArgs &a = b.args;
   a.items = reinterpret_cast<const MixItem *>(base + o_items);
   a.jobs = reinterpret_cast<const MixJob *>(base + o_jobs);

@@ -19,12 +19,24 @@ struct MixDeleter {
 };
 using MixPtr = std::unique_ptr<MixBatch, MixDeleter>;
 
+// A caller-owned device buffer for the work rows of one-shot batches on one
+// stream, reused from batch to batch and grown (in that stream's order) only
+// when a batch needs more.  Allocating hundreds of MB per batch instead was
+// measured to block the building thread for up to hundreds of milliseconds
+// while other streams' kernels ran.  The owner frees `ptr` after the stream's
+// work has finished.
+struct ScratchSlot {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+
 // Prepare a mixed batch; `forced` (optional) gives every op's plan.
 // With `ordered`, the batch is a one-shot, stream-ordered batch for that
 // stream (no graph): its device memory is allocated and freed in the stream's
-// order and building it never synchronizes the device.
+// order and building it never synchronizes the device; `scratch` (optional,
+// one-shot batches) supplies its work rows.
 int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, const rsgpu_mix_options &opt,
-              MixPtr &out, cudaStream_t ordered = nullptr);
+              MixPtr &out, cudaStream_t ordered = nullptr, ScratchSlot *scratch = nullptr);
 // The validation mix_build applies to each operation (reference error
 // precedence; shard pointers must be non-null).
 int mix_validate(const rsgpu_mix_op &o, int device);

@@ -39,7 +39,7 @@ struct UploadSlot {
 // A small ring per thread, so an upload waits only for the copy issued
 // kUploadSlots uploads earlier (a call that uploads tables and then its job
 // blob does not wait for its own first copy).
-constexpr int kUploadSlots = 4;
+constexpr int kUploadSlots = 8;
 thread_local UploadSlot t_upload[kUploadSlots];
 thread_local int t_upload_next = 0;
 
@@ -54,7 +54,10 @@ int upload(const void *src, size_t bytes, void **dev, cudaStream_t s) {
   if (u.cap < bytes) {
     if (u.host) cudaFreeHost(u.host);
     u.host = nullptr;
-    size_t cap = std::max<size_t>(bytes, 1 << 20);
+    // Geometric growth: freeing pinned memory synchronizes the device, so it
+    // should happen a handful of times per thread, not per call.
+    size_t cap = std::max<size_t>(u.cap * 2, 1 << 20);
+    while (cap < bytes) cap <<= 1;
     RS_CUDA(cudaHostAlloc(&u.host, cap, cudaHostAllocDefault));
     u.cap = cap;
   }

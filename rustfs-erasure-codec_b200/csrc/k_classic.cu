@@ -18,6 +18,7 @@
 #include "apply_tile.cuh"
 #include "common.hpp"
 #include "kernels.hpp"
+#include "launch_cfg.hpp"
 
 namespace rsgpu {
 
@@ -415,11 +416,9 @@ template <int V, int S, bool VERIFY>
 void launch_tma(const ApplyArgs &a, cudaStream_t s) {
   constexpr size_t smem = size_t(S) * 4 * kApplyThreads * kApplyVec * V;
   static int grid_max = 0;
-  if (!grid_max) {
-    const void *fn = (const void *)k_apply_tma<V, S, VERIFY>;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    grid_max = grid_for(fn, kApplyThreads + 32, smem);
-  }
+  const void *fn = (const void *)k_apply_tma<V, S, VERIFY>;
+  ensure_smem_limit(fn, smem);  // per device, set once
+  if (!grid_max) grid_max = grid_for(fn, kApplyThreads + 32, smem);
   const uint64_t tile = uint64_t(kApplyThreads) * kApplyVec * V;
   const uint64_t tiles = ((a.len + tile - 1) / tile) * a.n_jobs;
   const int grid = int(tiles < uint64_t(grid_max) ? tiles : grid_max);
@@ -484,11 +483,8 @@ cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cud
 cudaError_t launch_decode_tables(const DecodeTableArgs &a, int n_tasks, int max_out, cudaStream_t s) {
   if (n_tasks == 0) return cudaSuccess;
   const size_t smem = size_t(a.k) * 2 * a.k + size_t(max_out) * a.k;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_decode_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(smem));
-    if (e != cudaSuccess) return e;
-  }
+  cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(k_decode_tables), smem);
+  if (e != cudaSuccess) return e;
   k_decode_tables<<<n_tasks, 256, smem, s>>>(a);
   launch_counter_add(1);
   return cudaGetLastError();

@@ -36,6 +36,7 @@
 #include "codec.hpp"
 #include "leo_fft.cuh"
 #include "leo_tile.cuh"
+#include "launch_cfg.hpp"
 #include "leopard.hpp"
 
 namespace rsgpu {
@@ -571,9 +572,9 @@ int configure_fft(const K kernel, const K2 kernel_wide, LeoLaunch &L, uint32_t r
       L.threads = 2 * kFftThreads;
       fn = reinterpret_cast<const void *>(kernel_wide);
     }
-    if (smem > 48 * 1024) RS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    RS_CUDA(ensure_smem_limit(fn, smem));
     int per_sm = 0;
-    RS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, L.threads, smem));
+    RS_CUDA(blocks_per_sm(fn, L.threads, smem, &per_sm));
     L.grid = int(std::min<uint64_t>(tiles, uint64_t(std::max(per_sm, 1)) * sm_count()));
   } else {
     // Work rows in a global slab (L2-resident): one 512-thread CTA per SM
@@ -602,9 +603,9 @@ int configure(const K kernel, LeoLaunch &L, uint32_t lanes, size_t len, uint64_t
   L.args.lanes = lanes;
   if (!L.global_work) {
     L.smem = smem;
-    if (smem > 48 * 1024) RS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    RS_CUDA(ensure_smem_limit(reinterpret_cast<const void *>(kernel), smem));
     int per_sm = 0;
-    RS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kLeoThreads, smem));
+    RS_CUDA(blocks_per_sm(reinterpret_cast<const void *>(kernel), kLeoThreads, smem, &per_sm));
     L.grid = int(std::min<uint64_t>(tiles, uint64_t(std::max(per_sm, 1)) * sm_count()));
   } else {
     // Work rows in a device slab: one region per resident CTA.
@@ -678,7 +679,7 @@ int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>
   const int bits = st.field->bits;
   const size_t smem = size_t(1u << bits) * 2;
   if (bits == 16) {
-    RS_CUDA(cudaFuncSetAttribute(k_leo_locator<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    RS_CUDA(ensure_smem_limit(reinterpret_cast<const void *>(k_leo_locator<16>), smem));
     k_leo_locator<16><<<int(pending.size()), 1024, smem, s>>>(
         static_cast<const uint8_t *const *>(d_pp), static_cast<uint16_t *const *>(d_oo), st.field->d_walsh,
         uint32_t(c.k), uint32_t(c.m), st.m, st.n);

@@ -71,6 +71,7 @@ struct Flight {
   cudaEvent_t done = nullptr;
   uint32_t *h_flags = nullptr;  // pinned, one word per request
   size_t h_cap = 0;
+  ScratchSlot scratch;  // work rows of this flight's batches
   bool busy = false;
 };
 
@@ -116,6 +117,7 @@ class Server {
     cv_.notify_all();
     if (worker_.joinable()) worker_.join();
     for (auto &f : flights_) {
+      if (f.scratch.ptr) cudaFreeAsync(f.scratch.ptr, f.stream);
       if (f.stream) cudaStreamSynchronize(f.stream);
       if (f.done) cudaEventDestroy(f.done);
       if (f.stream) cudaStreamDestroy(f.stream);
@@ -328,7 +330,7 @@ class Server {
       rsgpu_mix_options_default(&mo);
       mo.planner = opt_.planner;
       mo.graph = 0;
-      rc = mix_build(ops.data(), ops.size(), nullptr, mo, b, f.stream);
+      rc = mix_build(ops.data(), ops.size(), nullptr, mo, b, f.stream, &f.scratch);
     }
     if (rc == RSGPU_OK) rc = mix_launch(*b, f.stream);
     if (rc == RSGPU_OK) {

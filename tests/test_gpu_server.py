@@ -163,3 +163,66 @@ def test_server_errors(rs, torch, codecs):
         srv.submit(c, "reconstruct", [ok[i] for i in range(48)], 64, present=pres)
     assert e.value.name == "TooFewShardsPresent"
     srv.close()
+
+
+def test_repeated_leopard_pattern_fft_then_dense_map(rs, torch, codecs):
+    # A Leopard GF(2^8) rebuild the plan table sends to the dense map: the
+    # server's batches run the FFT decode until the pattern is due under the
+    # per-call rule, then derive its map and use it.  Every result must equal
+    # the oracle, whichever path ran, alone or beside other batches.
+    from rsgpu import tune_mix
+
+    g = ("leopard_gf8", 32, 16)
+    c = codecs[g]
+    k, m = 32, 16
+    rng = np.random.default_rng(31)
+    pres = np.ones(k + m, np.uint8)
+    pres[rng.choice(k + m, size=4, replace=False)] = 0
+    rs.Tuner.clear()
+    rs.Tuner.load(tune_mix.DEFAULT_TABLE)
+    try:
+        size = None
+        for cand in (1 << 20, 2 << 20, 4 << 20):
+            op = dict(codec=c, op="reconstruct", shards=[0] * (k + m), shard_len=cand, present=pres, goal="all")
+            p = rs.Tuner.lookup(op)
+            if p is not None and p[0] == 0:
+                size = cand
+                break
+        if size is None:
+            pytest.skip("the plan table keeps 32+16 rebuilds on the FFT decode")
+        data = rng.integers(0, 256, (k + m, size), dtype=np.uint8)
+        want, _ = oracle_apply(g, c, "reconstruct", data, pres, "all")
+        srv = rs.Server(streams=2, max_batch=4, planner="model")
+        for call in range(5):  # one at a time
+            t = torch.from_numpy(data).cuda()
+            t[torch.from_numpy(pres == 0).cuda()] = 0
+            srv.submit(c, "reconstruct", [t[j] for j in range(k + m)], size, present=pres, tag=call + 1)
+            comp = srv.wait(1)
+            assert comp[0]["status"] == 0
+            assert np.array_equal(t.cpu().numpy(), want), call
+            torch.cuda.synchronize()
+        srv.close()
+        # Several new patterns at once, one request per batch, built while
+        # earlier batches run.
+        pats = []
+        for _ in range(3):
+            p2 = np.ones(k + m, np.uint8)
+            p2[rng.choice(k + m, size=3, replace=False)] = 0
+            pats.append(p2)
+        wants = [oracle_apply(g, c, "reconstruct", data, p2, "all")[0] for p2 in pats]
+        srv = rs.Server(streams=3, max_batch=1, planner="model")
+        for rnd in range(3):
+            bufs = []
+            for i, p2 in enumerate(pats):
+                t = torch.from_numpy(data).cuda()
+                t[torch.from_numpy(p2 == 0).cuda()] = 0
+                bufs.append(t)
+                srv.submit(c, "reconstruct", [t[j] for j in range(k + m)], size, present=p2, tag=10 * rnd + i + 1)
+            comps = srv.wait(len(pats))
+            assert all(x["status"] == 0 for x in comps)
+            torch.cuda.synchronize()
+            for i, t in enumerate(bufs):
+                assert np.array_equal(t.cpu().numpy(), wants[i]), (rnd, i)
+        srv.close()
+    finally:
+        rs.Tuner.clear()
