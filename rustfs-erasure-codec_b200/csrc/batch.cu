@@ -288,7 +288,7 @@ struct MixBatch {
   }
   template <class T>
   cudaError_t alloc(T **p, size_t bytes) {
-    return stream_ordered ? cudaMallocAsync(reinterpret_cast<void **>(p), bytes, stream)
+    return stream_ordered ? cudaError_t(lib_malloc_async(reinterpret_cast<void **>(p), bytes, stream))
                           : cudaMalloc(reinterpret_cast<void **>(p), bytes);
   }
 
@@ -759,7 +759,7 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
         scratch->ptr = nullptr;
         scratch->bytes = 0;
         const size_t want = need + need / 4;
-        RS_CUDA(cudaMallocAsync(&scratch->ptr, want, b.stream));
+        RS_CUDA(cudaError_t(lib_malloc_async(&scratch->ptr, want, b.stream)));
         scratch->bytes = want;
       }
       b.d_scratch = static_cast<uint32_t *>(scratch->ptr);

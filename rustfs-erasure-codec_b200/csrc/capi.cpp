@@ -73,29 +73,13 @@ int ensure_io(rsgpu_codec *h) {
 
 size_t round16(size_t n) { return (n + 15) & ~size_t(15); }
 
-// Staging memory of host-memory calls comes from a pool private to this
-// library (one per device), which keeps up to 1 GiB of freed memory mapped
-// between calls: the device's default pool gives freed memory back at every
-// synchronisation, so each call would map its staging area afresh.  A private
-// pool leaves the default pool's settings (which other code in the process
-// may rely on) untouched.
+// Staging memory of host-memory calls comes from the library's own pool
+// (lib_pool), which keeps freed memory mapped between calls.
 int staging_pool(int device, cudaMemPool_t *out) {
-  static std::mutex mu;
-  static std::vector<cudaMemPool_t> pools;
-  std::lock_guard<std::mutex> g(mu);
-  if (pools.size() <= size_t(device)) pools.resize(size_t(device) + 1, nullptr);
-  if (!pools[device]) {
-    cudaMemPoolProps props{};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = device;
-    cudaMemPool_t p = nullptr;
-    RS_CUDA(cudaMemPoolCreate(&p, &props));
-    uint64_t keep = 1ull << 30;
-    RS_CUDA(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep));
-    pools[device] = p;
-  }
-  *out = pools[device];
+  (void)device;  // the pool of the current device
+  void *p = nullptr;
+  RS_CUDA(cudaError_t(rsgpu::lib_pool(&p)));
+  *out = static_cast<cudaMemPool_t>(p);
   return RSGPU_OK;
 }
 
@@ -234,7 +218,7 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
   // The other families report per chunk.
   uint32_t *vflags = nullptr;
   if (op == OP_VERIFY && c.family == RSGPU_FAMILY_CLASSIC && c.field == RSGPU_FIELD_GF8) {
-    RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&vflags), std::max<size_t>(n_stripes, 1) * 4, h->io[0]));
+    RS_CUDA(cudaError_t(rsgpu::lib_malloc_async(reinterpret_cast<void **>(&vflags), std::max<size_t>(n_stripes, 1) * 4, h->io[0])));
     RS_CUDA(cudaMemsetAsync(vflags, 0, std::max<size_t>(n_stripes, 1) * 4, h->io[0]));
     RS_CUDA(cudaEventRecord(ev, h->io[0]));
     RS_CUDA(cudaStreamWaitEvent(h->io[1], ev, 0));

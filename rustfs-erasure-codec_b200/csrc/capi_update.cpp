@@ -62,7 +62,7 @@ int apply_host(Codec &c, const std::vector<const uint8_t *> &in, const std::vect
   UP_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   uint8_t *d = nullptr;
   const size_t pitch = (len + 255) & ~size_t(255);
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&d), (n_in + m) * pitch, s);
+  cudaError_t e = cudaError_t(rsgpu::lib_malloc_async(reinterpret_cast<void **>(&d), (n_in + m) * pitch, s));
   int rc = e == cudaSuccess ? RSGPU_OK : rsgpu::cuda_status(e);
   std::vector<const uint8_t *> din(n_in);
   std::vector<uint8_t *> dpar(m);

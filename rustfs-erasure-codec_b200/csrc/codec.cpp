@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace rsgpu {
 
@@ -43,6 +45,40 @@ constexpr int kUploadSlots = 8;
 thread_local UploadSlot t_upload[kUploadSlots];
 thread_local int t_upload_next = 0;
 
+}  // namespace
+
+int lib_pool(void **out) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return int(e);
+  std::lock_guard<std::mutex> g(mu);
+  auto it = pools.find(dev);
+  if (it == pools.end()) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if ((e = cudaMemPoolCreate(&p, &props)) != cudaSuccess) return int(e);
+    uint64_t keep = 2ull << 30;
+    if ((e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return int(e);
+    it = pools.emplace(dev, p).first;
+  }
+  *out = it->second;
+  return int(cudaSuccess);
+}
+
+int lib_malloc_async(void **p, size_t bytes, void *stream) {
+  void *pool = nullptr;
+  int e = lib_pool(&pool);
+  if (e != int(cudaSuccess)) return e;
+  return int(cudaMallocFromPoolAsync(p, bytes, static_cast<cudaMemPool_t>(pool), static_cast<cudaStream_t>(stream)));
+}
+
+namespace {
+
 // Copies `bytes` of host data to a fresh stream-ordered device allocation
 // through a pinned, event-guarded bounce buffer.  The device block is freed
 // stream-ordered by the caller.
@@ -62,7 +98,7 @@ int upload(const void *src, size_t bytes, void **dev, cudaStream_t s) {
     u.cap = cap;
   }
   std::memcpy(u.host, src, bytes);
-  RS_CUDA(cudaMallocAsync(dev, std::max<size_t>(bytes, 16), s));
+  RS_CUDA(cudaError_t(lib_malloc_async(dev, std::max<size_t>(bytes, 16), s)));
   RS_CUDA(cudaMemcpyAsync(*dev, u.host, bytes, cudaMemcpyHostToDevice, s));
   RS_CUDA(cudaEventRecord(u.done, s));
   return RSGPU_OK;
@@ -259,7 +295,7 @@ int Codec::decode_tables(const std::vector<const ClassicPlan *> &plans, std::vec
     int rc = upload(tasks.data(), tasks.size() * sizeof(DecodeTask), &d_tasks, s);
     if (rc) return rc;
     int *d_status = nullptr;
-    RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&d_status), tasks.size() * sizeof(int), s));
+    RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&d_status), tasks.size() * sizeof(int), s)));
     DecodeTableArgs a;
     a.tasks = static_cast<const DecodeTask *>(d_tasks);
     a.matrix = d_matrix;
@@ -441,7 +477,7 @@ int Codec::verify_dev(size_t n_stripes, const uint8_t *const *shards, size_t len
   if (tbl)
     for (auto &j : jobs) j.tbl = tbl;
   uint32_t *flags = nullptr;
-  RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&flags), n_stripes * 4, s));
+  RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&flags), n_stripes * 4, s)));
   RS_CUDA(cudaMemsetAsync(flags, 0, n_stripes * 4, s));
   int rc = run_apply(jobs, ptrs, len, true, flags, s);
   if (rc) return rc;

@@ -45,4 +45,18 @@ inline size_t packed_table_words(size_t n_out, size_t n_in) {
 
 uint64_t launch_counter_add(uint64_t n);
 
+// Stream-ordered device memory from the library's own pool on the current
+// device, which keeps up to 2 GiB of freed memory mapped between calls (the
+// device's default pool gives freed memory back at every synchronization,
+// so each call would map it afresh: host time that varied fivefold between
+// passes of the same per-stripe calls).  Released with cudaFreeAsync.
+// Returns a cudaError_t value.
+int lib_malloc_async(void **p, size_t bytes, void *stream);
+template <class T>
+inline int lib_malloc_async(T **p, size_t bytes, void *stream) {
+  return lib_malloc_async(reinterpret_cast<void **>(p), bytes, stream);
+}
+// The pool itself (cudaMemPool_t), for cudaMallocFromPoolAsync callers.
+int lib_pool(void **out);
+
 }  // namespace rsgpu

@@ -663,7 +663,7 @@ int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>
   for (size_t i = 0; i < pending.size(); ++i) std::memcpy(&pres[i * total], pending[i].first.data(), total);
   // Stream-ordered scratch: nothing here waits for other streams' work.
   uint8_t *d_pres = nullptr;
-  RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&d_pres), pres.size(), s));
+  RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&d_pres), pres.size(), s)));
   RS_CUDA(cudaMemcpyAsync(d_pres, pres.data(), pres.size(), cudaMemcpyHostToDevice, s));
   std::vector<const uint8_t *> pp(pending.size());
   std::vector<uint16_t *> oo(pending.size());
@@ -672,8 +672,8 @@ int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>
     oo[i] = st.plans[pending[i].first].err;
   }
   void *d_pp = nullptr, *d_oo = nullptr;
-  RS_CUDA(cudaMallocAsync(&d_pp, pp.size() * sizeof(void *), s));
-  RS_CUDA(cudaMallocAsync(&d_oo, oo.size() * sizeof(void *), s));
+  RS_CUDA(cudaError_t(lib_malloc_async(&d_pp, pp.size() * sizeof(void *), s)));
+  RS_CUDA(cudaError_t(lib_malloc_async(&d_oo, oo.size() * sizeof(void *), s)));
   RS_CUDA(cudaMemcpyAsync(d_pp, pp.data(), pp.size() * sizeof(void *), cudaMemcpyHostToDevice, s));
   RS_CUDA(cudaMemcpyAsync(d_oo, oo.data(), oo.size() * sizeof(void *), cudaMemcpyHostToDevice, s));
   const int bits = st.field->bits;
@@ -787,7 +787,7 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
   std::memcpy(blob.data() + jb, shards, pb);
   std::memcpy(blob.data() + jb + pb, roles.data(), roles.size());
   if (one_shot) {
-    RS_CUDA(cudaMallocAsync(&L.d_blob, std::max<size_t>(blob.size(), 16), s));
+    RS_CUDA(cudaError_t(lib_malloc_async(&L.d_blob, std::max<size_t>(blob.size(), 16), s)));
     L.blob_ordered = true;
     L.blob_stream = s;
   } else {
@@ -1012,7 +1012,7 @@ int leopard_verify(Codec &c, size_t n, const uint8_t *const *shards, size_t len,
     return c.verify_dev(n, shards, len, ok, s, tbl);
   }
   uint32_t *flags = nullptr;
-  RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&flags), std::max<size_t>(n, 1) * 4, s));
+  RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&flags), std::max<size_t>(n, 1) * 4, s)));
   RS_CUDA(cudaMemsetAsync(flags, 0, std::max<size_t>(n, 1) * 4, s));
   int rc = run_once(c, RSGPU_OP_VERIFY, n, const_cast<uint8_t *const *>(shards), nullptr, len, 0, nullptr, 0, flags, s);
   std::vector<uint32_t> f(n);
@@ -1269,7 +1269,7 @@ int leopard_dense_encode(Codec &c, std::vector<uint8_t> &rows) {
   cudaStream_t s = nullptr;
   RS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   uint8_t *d = nullptr;
-  int rc = cuda_status(cudaMallocAsync(reinterpret_cast<void **>(&d), host.size(), s));
+  int rc = cuda_status(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&d), host.size(), s)));
   if (rc == RSGPU_OK) rc = cuda_status(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, s));
   std::vector<uint8_t *> ptrs(total);
   for (size_t i = 0; i < total; ++i) ptrs[i] = d + i * L;
@@ -1325,7 +1325,7 @@ int derive_dense8(Codec &c, size_t n, const uint8_t *present, int goal, std::vec
     for (size_t q = 0; q < maps[i].inputs.size(); ++q) host[(i * total + maps[i].inputs[q]) * L + q] = one;
   // Stream-ordered on `s`; the host waits for `s` only, to read the maps.
   uint8_t *d = nullptr;
-  RS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&d), host.size(), s));
+  RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&d), host.size(), s)));
   int rc = cuda_status(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, s));
   std::vector<uint8_t *> ptrs(n * total);
   for (size_t i = 0; i < n * total; ++i) ptrs[i] = d + i * L;

@@ -32,6 +32,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -75,6 +76,33 @@ struct Flight {
   bool busy = false;
 };
 
+// Work-row buffers of stopped servers, by device, for the next server to
+// take: a buffer grows to the widest batch it has served (hundreds of MB for
+// wide GF(2^16) decodes), and growing it again in every new server put that
+// allocation, which can block for up to hundreds of milliseconds, on some
+// request's path.  Buffers are returned only after their stream has
+// finished, so a later stream may use them at once.
+std::mutex g_slots_mu;
+std::map<int, std::vector<ScratchSlot>> g_slots;
+
+ScratchSlot take_slot(int device) {
+  std::lock_guard<std::mutex> g(g_slots_mu);
+  auto &v = g_slots[device];
+  if (v.empty()) return ScratchSlot{};
+  auto best = std::max_element(v.begin(), v.end(), [](const ScratchSlot &x, const ScratchSlot &y) {
+    return x.bytes < y.bytes;
+  });
+  ScratchSlot out = *best;
+  v.erase(best);
+  return out;
+}
+
+void return_slot(int device, const ScratchSlot &s) {
+  if (!s.ptr) return;
+  std::lock_guard<std::mutex> g(g_slots_mu);
+  g_slots[device].push_back(s);
+}
+
 }  // namespace
 
 class Server {
@@ -92,16 +120,11 @@ class Server {
     if (opt_.max_inflight == 0) opt_.max_inflight = 4096;
     if (opt_.max_batch == 0) opt_.max_batch = 1024;
     if (opt_.streams == 0) opt_.streams = 3;
-    // Stream-ordered staging: keep freed blocks in the pool instead of
-    // returning them to the driver at every synchronization.
-    cudaMemPool_t pool;
-    SV_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
-    uint64_t keep = opt_.device_budget;
-    SV_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     flights_.resize(opt_.streams);
     for (auto &f : flights_) {
       SV_CUDA(cudaStreamCreateWithFlags(&f.stream, cudaStreamNonBlocking));
       SV_CUDA(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
+      f.scratch = take_slot(device_);
     }
     t0_ = Clock::now();
     worker_ = std::thread([this] { loop(); });
@@ -117,8 +140,9 @@ class Server {
     cv_.notify_all();
     if (worker_.joinable()) worker_.join();
     for (auto &f : flights_) {
-      if (f.scratch.ptr) cudaFreeAsync(f.scratch.ptr, f.stream);
       if (f.stream) cudaStreamSynchronize(f.stream);
+      return_slot(device_, f.scratch);  // its stream has finished
+      f.scratch = ScratchSlot{};
       if (f.done) cudaEventDestroy(f.done);
       if (f.stream) cudaStreamDestroy(f.stream);
       if (f.h_flags) cudaFreeHost(f.h_flags);
@@ -311,7 +335,7 @@ class Server {
       if (q->r.mem == RSGPU_MEM_DEVICE) {
         q->dev = q->shards;
       } else {
-        if (cudaMallocAsync(reinterpret_cast<void **>(&q->staging), total * len, f.stream) != cudaSuccess) {
+        if (cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&q->staging), total * len, f.stream)) != cudaSuccess) {
           rc = RSGPU_ERR_OUT_OF_MEMORY;
           break;
         }
