@@ -126,6 +126,18 @@ class Server {
       SV_CUDA(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
       f.scratch = take_slot(device_);
     }
+    // Every stream starts with a work-row buffer as large as the largest one
+    // handed over, so that no stream grows its own (a pool allocation of up
+    // to a few hundred MB) under its first wide batch, on a request's path.
+    size_t widest = 0;
+    for (auto &f : flights_) widest = std::max(widest, f.scratch.bytes);
+    for (auto &f : flights_) {
+      if (f.scratch.bytes >= widest) continue;
+      if (f.scratch.ptr) SV_CUDA(cudaFreeAsync(f.scratch.ptr, f.stream));
+      f.scratch = ScratchSlot{};
+      SV_CUDA(cudaError_t(lib_malloc_async(&f.scratch.ptr, widest, f.stream)));
+      f.scratch.bytes = widest;
+    }
     t0_ = Clock::now();
     worker_ = std::thread([this] { loop(); });
     return RSGPU_OK;

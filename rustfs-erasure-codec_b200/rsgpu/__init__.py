@@ -178,6 +178,19 @@ SZP = ctypes.POINTER(ctypes.c_size_t)
 U8P = ctypes.POINTER(ctypes.c_uint8)
 
 
+def _free_handle(owner, fn_name: str) -> None:
+    """Release owner._h through the named C-ABI free call.  Safe from __del__
+    during interpreter shutdown, when module globals may already be gone."""
+    h = getattr(owner, "_h", None)
+    if not h:
+        return
+    lib = _L
+    fn = getattr(lib, fn_name, None) if lib is not None else None
+    if fn is not None:
+        fn(h)
+    owner._h = None
+
+
 def _lib():
     global _L
     if _L is None:
@@ -408,9 +421,7 @@ class VerifyWorkspace:
         self._h = h
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            _lib().rsgpu_verify_ws_free(self._h)
-            self._h = None
+        _free_handle(self, "rsgpu_verify_ws_free")
 
 
 class ReconstructWorkspace:
@@ -426,9 +437,7 @@ class ReconstructWorkspace:
         return list(out)[:n]
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            _lib().rsgpu_reconstruct_ws_free(self._h)
-            self._h = None
+        _free_handle(self, "rsgpu_reconstruct_ws_free")
 
 
 OP = {"encode": 0, "reconstruct": 1, "verify": 2}
@@ -475,10 +484,7 @@ class PreparedBatch:
         return int(_lib().rsgpu_batch_kernel_count(self._h))
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h and _L is not None and getattr(_L, "rsgpu_batch_free", None) is not None:
-            _L.rsgpu_batch_free(h)
-            self._h = None
+        _free_handle(self, "rsgpu_batch_free")
 
 
 def _mix_ops(ops, keep):
@@ -559,10 +565,7 @@ class MixedBatch:
         return [parr[i].tuple() for i in range(self.n_ops)]
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h and _L is not None and getattr(_L, "rsgpu_mix_free", None) is not None:
-            _L.rsgpu_mix_free(h)
-            self._h = None
+        _free_handle(self, "rsgpu_mix_free")
 
 
 class _StreamIO:
@@ -871,9 +874,7 @@ class ReedSolomon:
         return cls(data_shards, parity_shards, options, field=field, _custom=rows)
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            _lib().rsgpu_codec_free(self._h)
-            self._h = None
+        _free_handle(self, "rsgpu_codec_free")
 
     def data_shard_count(self) -> int:
         return _lib().rsgpu_data_shard_count(self._h)

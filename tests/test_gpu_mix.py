@@ -187,6 +187,26 @@ def test_mix_every_plan_writes_the_same_bytes(rs, torch, codecs, variant):
     assert list(mb.results()) == flags
 
 
+@pytest.mark.parametrize("size,want_tile", [(4096, 1), (196608, 3)])
+def test_small_batch_runs_transforms_at_the_finest_tile(rs, torch, codecs, size, want_tile):
+    # The fixed rule gives a 128+64 encode 8 blocks per work item.  A batch
+    # with fewer items than the kernel's resident CTAs (one 4 KiB stripe: 8
+    # items) runs at the finest tile instead, so more items run side by side;
+    # one that fills the GPU (192 KiB: 384 items) keeps the planned tile.
+    # The bytes are the oracle's either way.
+    g = ("leopard_gf8", 128, 64)
+    c = codecs[g]
+    k, m = 128, 64
+    data = np.random.default_rng(size).integers(0, 256, (k + m, size), dtype=np.uint8)
+    t = torch.from_numpy(data).cuda()
+    op = dict(codec=c, op="encode", shards=[t[j] for j in range(k + m)], shard_len=size)
+    mb = rs.MixedBatch([op], planner="fixed", graph=False)
+    assert mb.plans() == [(rs.ALGO_FFT, want_tile)]
+    mb.launch()
+    torch.cuda.synchronize()
+    assert np.array_equal(t.cpu().numpy(), oracle_encode(g, c, data))
+
+
 def test_mix_dense_leopard_maps_are_exact_on_non_codewords(rs, torch, codecs):
     # Leopard GF(2^8) operations run as dense matrices over the Leopard field:
     # the reconstruction map uses every present shard, like the FFT decode, so
