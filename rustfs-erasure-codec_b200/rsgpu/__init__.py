@@ -180,7 +180,8 @@ U8P = ctypes.POINTER(ctypes.c_uint8)
 
 def _free_handle(owner, fn_name: str) -> None:
     """Release owner._h through the named C-ABI free call.  Safe from __del__
-    during interpreter shutdown, when module globals may already be gone."""
+    during interpreter shutdown, when module globals may already be gone
+    (callers bind this function as a default argument for that reason)."""
     h = getattr(owner, "_h", None)
     if not h:
         return
@@ -420,8 +421,8 @@ class VerifyWorkspace:
         _check(_lib().rsgpu_verify_ws_new(codec._h, shard_len, ctypes.byref(h)))
         self._h = h
 
-    def __del__(self):
-        _free_handle(self, "rsgpu_verify_ws_free")
+    def __del__(self, _free=_free_handle):
+        _free(self, "rsgpu_verify_ws_free")
 
 
 class ReconstructWorkspace:
@@ -436,8 +437,8 @@ class ReconstructWorkspace:
         _lib().rsgpu_reconstruct_ws_targets(self._h, out, n)
         return list(out)[:n]
 
-    def __del__(self):
-        _free_handle(self, "rsgpu_reconstruct_ws_free")
+    def __del__(self, _free=_free_handle):
+        _free(self, "rsgpu_reconstruct_ws_free")
 
 
 OP = {"encode": 0, "reconstruct": 1, "verify": 2}
@@ -483,8 +484,8 @@ class PreparedBatch:
     def kernel_count(self) -> int:
         return int(_lib().rsgpu_batch_kernel_count(self._h))
 
-    def __del__(self):
-        _free_handle(self, "rsgpu_batch_free")
+    def __del__(self, _free=_free_handle):
+        _free(self, "rsgpu_batch_free")
 
 
 def _mix_ops(ops, keep):
@@ -564,8 +565,8 @@ class MixedBatch:
         _check(_lib().rsgpu_mix_get_plans(self._h, ctypes.addressof(parr), self.n_ops))
         return [parr[i].tuple() for i in range(self.n_ops)]
 
-    def __del__(self):
-        _free_handle(self, "rsgpu_mix_free")
+    def __del__(self, _free=_free_handle):
+        _free(self, "rsgpu_mix_free")
 
 
 class _StreamIO:
@@ -873,8 +874,8 @@ class ReedSolomon:
         [X coefficient, constant])."""
         return cls(data_shards, parity_shards, options, field=field, _custom=rows)
 
-    def __del__(self):
-        _free_handle(self, "rsgpu_codec_free")
+    def __del__(self, _free=_free_handle):
+        _free(self, "rsgpu_codec_free")
 
     def data_shard_count(self) -> int:
         return _lib().rsgpu_data_shard_count(self._h)
