@@ -207,6 +207,54 @@ def test_small_batch_runs_transforms_at_the_finest_tile(rs, torch, codecs, size,
     assert np.array_equal(t.cpu().numpy(), oracle_encode(g, c, data))
 
 
+@pytest.mark.parametrize("plan", [None, 1, 2, 3])
+def test_mix_wide_gf16_code_with_global_work_rows(rs, torch, plan):
+    # GF(2^16) 600+300: 1024 encode rows and 2048 decode lanes, more than a
+    # k_mix CTA's shared memory holds, so the work rows live in the batch's
+    # global scratch.  Encode, rebuild (goals all and data), and verify of a
+    # codeword and of a corrupted stripe in one batch, at the planner's tile
+    # (None) and at every forced tile, against the oracle on inputs that are
+    # not codewords.
+    geom = ("leopard_gf16", 600, 300)
+    k, m = geom[1], geom[2]
+    total = k + m
+    cods = {geom: rs.ReedSolomon(k, m, rs.CodecOptions(codec_family="leopard_gf16"))}
+    rng = np.random.default_rng(600 + (plan or 0))
+    specs, host = [], []
+    for op, length, goal in [("encode", 2048, "all"), ("reconstruct", 1024, "all"), ("reconstruct", 3072, "data"),
+                             ("verify", 1024, "all"), ("verify", 2048, "all")]:
+        data = rng.integers(0, 256, (total, length), dtype=np.uint8)
+        present = None
+        if op == "verify":
+            data = oracle_encode(geom, cods[geom], data)
+            if length == 2048:
+                data[k + 7, 100] ^= 0x40
+        if op == "reconstruct":
+            present = np.ones(total, np.uint8)
+            present[rng.choice(total, size=m, replace=False)] = 0
+        specs.append(dict(geom=geom, op=op, present=present, goal=goal, len=length))
+        host.append(data)
+    offs, cur = [], 0
+    for d in host:
+        offs.append(cur)
+        cur += (d.size + 255) // 256 * 256
+    arena = torch.zeros(cur + 256, dtype=torch.uint8, device="cuda")
+    for o, d in zip(offs, host):
+        arena[o:o + d.size] = torch.from_numpy(d.reshape(-1)).cuda()
+    ops = [dict(codec=cods[geom], op=sp["op"], shard_len=sp["len"], present=sp["present"], goal=sp["goal"],
+                shards=[arena.data_ptr() + o + j * sp["len"] for j in range(total)]) for sp, o in zip(specs, offs)]
+    exp, flags = oracle_expect(specs, host, cods)
+    assert flags == [True, True, True, True, False]
+    plans = None if plan is None else [(rs.ALGO_FFT, plan)] * len(ops)
+    mb = rs.MixedBatch(ops, plans=plans, graph=False)
+    if plan is None:  # a small batch: the finest tile
+        assert mb.plans() == [(rs.ALGO_FFT, 1)] * len(ops)
+    mb.launch()
+    torch.cuda.synchronize()
+    check(torch, arena, offs, exp, specs, f"tile {plan}")
+    assert list(mb.results()) == flags
+
+
 def test_mix_dense_leopard_maps_are_exact_on_non_codewords(rs, torch, codecs):
     # Leopard GF(2^8) operations run as dense matrices over the Leopard field:
     # the reconstruction map uses every present shard, like the FFT decode, so
