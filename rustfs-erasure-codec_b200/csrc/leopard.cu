@@ -1409,14 +1409,14 @@ constexpr size_t kNaLanes = RSGPU_NOALLOC_MAX_LANES;
 constexpr size_t kNaScratchWords = RSGPU_NOALLOC_SCRATCH_BYTES / 4;
 static_assert(RSGPU_NOALLOC_SCRATCH_BYTES >= kNaLanes * 64, "one CTA at the lane limit must fit");
 
-__device__ __align__(256) uint32_t na_scratch[kNaScratchWords];  // work rows, one region per CTA
-__device__ __align__(256) const uint8_t *na_ptrs[kNaLanes];      // shard pointers (k + p <= lanes)
-__device__ __align__(256) uint8_t na_present[kNaLanes];
-__device__ __align__(256) uint8_t na_role[kNaLanes];
-__device__ __align__(256) uint16_t na_err[kNaLanes];
-__device__ __align__(256) LeoJob na_job;
-__device__ __align__(256) const uint8_t *na_present_ref[1];
-__device__ __align__(256) uint16_t *na_err_ref[1];
+static __device__ __align__(256) uint32_t na_scratch[kNaScratchWords];  // work rows, one region per CTA
+static __device__ __align__(256) const uint8_t *na_ptrs[kNaLanes];      // shard pointers (k + p <= lanes)
+static __device__ __align__(256) uint8_t na_present[kNaLanes];
+static __device__ __align__(256) uint8_t na_role[kNaLanes];
+static __device__ __align__(256) uint16_t na_err[kNaLanes];
+static __device__ __align__(256) LeoJob na_job;
+static __device__ __align__(256) const uint8_t *na_present_ref[1];
+static __device__ __align__(256) uint16_t *na_err_ref[1];
 
 struct NaDevice {
   bool ready = false;

@@ -129,14 +129,21 @@ class Server {
     // Every stream starts with a work-row buffer as large as the largest one
     // handed over, so that no stream grows its own (a pool allocation of up
     // to a few hundred MB) under its first wide batch, on a request's path.
+    // Best effort: a stream whose allocation fails starts empty and grows its
+    // buffer when a batch needs it, as it would without this step.
     size_t widest = 0;
     for (auto &f : flights_) widest = std::max(widest, f.scratch.bytes);
     for (auto &f : flights_) {
       if (f.scratch.bytes >= widest) continue;
       if (f.scratch.ptr) SV_CUDA(cudaFreeAsync(f.scratch.ptr, f.stream));
       f.scratch = ScratchSlot{};
-      SV_CUDA(cudaError_t(lib_malloc_async(&f.scratch.ptr, widest, f.stream)));
-      f.scratch.bytes = widest;
+      void *p = nullptr;
+      if (cudaError_t(lib_malloc_async(&p, widest, f.stream)) == cudaSuccess) {
+        f.scratch.ptr = p;
+        f.scratch.bytes = widest;
+      } else {
+        cudaGetLastError();  // an out-of-memory here is not sticky
+      }
     }
     t0_ = Clock::now();
     worker_ = std::thread([this] { loop(); });
