@@ -157,12 +157,14 @@ def profiled_traffic_ratio():
 def cpu_sample(threads):
     """Time the oracle's threaded GFNI/AVX2 restatement of the reference's
     fastest x86 classic path on a bounded sample: 64 stripes per geometry,
-    encode + rebuild (the same row kernel applied to recovery rows) + verify."""
+    encode + rebuild (the same row kernel applied to recovery rows) + verify.
+    Returns GB/s of algorithmic bytes, the kernel's name, the sample's stripes
+    per geometry and GiB/s in the reference's data-bytes convention."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
     n = 64
-    total_bytes = 0
+    total_bytes = data_bytes = 0
     t_total = 0.0
     for gi, (k, m) in enumerate(GEOMS):
         rng = np.random.default_rng(SEED + gi)
@@ -199,8 +201,9 @@ def cpu_sample(threads):
         t_ver = time.perf_counter() - t0
         assert ok
         total_bytes += eb + rb + vb
+        data_bytes += 3 * n * k * SHARD
         t_total += t_enc + t_rec + t_ver
-    return total_bytes / t_total / 1e9, O.fast_kernel_name(), n
+    return total_bytes / t_total / 1e9, O.fast_kernel_name(), n, data_bytes / t_total / 2**30
 
 
 def run_reference(args, rank, world):
@@ -209,17 +212,19 @@ def run_reference(args, rank, world):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    vals = []
+    vals, dvals = [], []
     for _ in range(args.warmup):
         cpu_sample(threads)
     for _ in range(args.steps):
-        v, kern, n = cpu_sample(threads)
+        v, kern, n, dv = cpu_sample(threads)
         vals.append(v)
+        dvals.append(dv)
     value = float(np.median(vals))
     line = {
         "impl": "reference", "metric": "batched classic encode+rebuild+verify GB/s (algorithmic bytes)",
         "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "data_gibs": round(float(np.median(dvals)), 3),
         "config": {"workload": "classic galois_8 10+4 and 16+4, 1 MiB shards, seeded erasures 1..m",
                    "stripes_per_geometry_per_step": n, "flush": "inputs larger than L2"},
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
@@ -414,6 +419,10 @@ def main():
     assert rsgpu.kernel_launch_count() - launches0 == gpu_launches
     ms_max = group.max(ms)
     value = total_bytes * world / (ms_max / 1e3) / 1e9
+    # The reference's own convention (data shards x shard bytes per operation,
+    # GiB/s; benches/throughput_matrix.rs:167-172): three operations per stripe.
+    data_bytes = sum(3 * w["n"] * w["k"] * SHARD for w in work)
+    data_gibs = data_bytes * world / (ms_max / 1e3) / 2**30
 
     # Dominant kernel (10+4 encode) timed alone with events on its stream.
     w0 = work[0]
@@ -513,8 +522,8 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, kern, n = cpu_sample(threads)
-        cpu = {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+        v, kern, n, dv = cpu_sample(threads)
+        cpu = {"value": round(v, 3), "unit": "GB/s", "data_gibs": round(dv, 3), "cores": threads, "kind": "port",
                "sample": f"{n} stripes per geometry: encode+rebuild+verify with the oracle's {kern} rows kernel"}
 
     if rank == 0:
@@ -522,6 +531,7 @@ def main():
             "metric": "batched classic encode+rebuild+verify GB/s (algorithmic bytes)",
             "value": round(value, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True,
+            "data_gibs": round(data_gibs, 1),
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": "classic galois_8 10+4 and 16+4, 1 MiB shards, seeded erasures 1..m",
                        "stripes_per_geometry": args.stripes, "ops_per_step": "encode, reconstruct, verify",
@@ -590,7 +600,8 @@ def config1_workload(torch, rsgpu, stream, gen):
     for name, b in (("encode", enc), ("reconstruct", rec), ("verify", ver)):
         med, p99 = _median_ms(torch, stream, b.launch, 20)
         out[name] = {"us": round(med * 1e3, 1), "p99_us": round(p99 * 1e3, 1),
-                     "gbs": round(nbytes / (med / 1e3) / 1e9, 1)}
+                     "gbs": round(nbytes / (med / 1e3) / 1e9, 1),
+                     "data_gibs": round(n * k * size / (med / 1e3) / 2**30, 1)}
     del buf, orig
     return out
 
@@ -630,6 +641,7 @@ def leopard16_workload(torch, rsgpu, stream, gen):
         med, p99 = _median_ms(torch, stream, b.launch, 10)
         out[name] = {"ms": round(med, 3), "p99_ms": round(p99, 3),
                      "gbs": round(nbytes / (med / 1e3) / 1e9, 1),
+                     "data_gibs": round(n * k * size / (med / 1e3) / 2**30, 1),
                      "mul_xor_per_s": float(f"{mx[name] / (med / 1e3):.4g}")}
     del buf, orig
     return out
