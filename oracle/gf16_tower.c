@@ -126,7 +126,7 @@ static int tinvert(size_t n, const t16 *in, t16 *out) {
 /* src/core/codec.rs:67-89 with nth(n) = [(n >> 8), n] (galois_16.rs:63-65). */
 int orc_gf16t_build_matrix(size_t k, size_t m, uint8_t *out) {
   size_t total = k + m;
-  t16 *v = (t16 *)malloc(total * k * sizeof(t16));
+  t16 *v = (t16 *)calloc(total * k + 1, sizeof(t16));
   t16 *inv = (t16 *)malloc(k * k * sizeof(t16));
   for (size_t r = 0; r < total; r++) {
     t16 a = {(uint8_t)(r >> 8), (uint8_t)r};
@@ -189,7 +189,7 @@ int orc_gf16t_reconstruct(size_t k, size_t m, const uint8_t *matrix, uint8_t *co
   if (!missing_any) return ORC_OK;
   if (np < k) return ORC_TOO_FEW_SHARDS_PRESENT;
   if (missing_data) {
-    t16 *sel = (t16 *)malloc(k * k * sizeof(t16));
+    t16 *sel = (t16 *)calloc(k * k + 1, sizeof(t16));
     t16 *dec = (t16 *)malloc(k * k * sizeof(t16));
     for (size_t r = 0; r < k; r++)
       for (size_t c = 0; c < k; c++) {

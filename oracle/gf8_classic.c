@@ -281,7 +281,7 @@ void orc_classic_encode(size_t k, size_t m, const uint8_t *matrix,
 int orc_classic_verify(size_t k, size_t m, const uint8_t *matrix,
                        const uint8_t *const *shards, size_t len) {
   uint8_t *scratch = (uint8_t *)malloc(m * len + 1);
-  uint8_t **par = (uint8_t **)malloc(m * sizeof(uint8_t *));
+  uint8_t **par = (uint8_t **)calloc(m + 1, sizeof(uint8_t *));
   for (size_t r = 0; r < m; r++) par[r] = scratch + r * len;
   orc_classic_encode(k, m, matrix, shards, par, len);
   int ok = 1;
