@@ -67,3 +67,38 @@ def test_argument_validation_precedes_device_use():
     with pytest.raises(rsgpu.RsError) as e:
         rsgpu.ReedSolomon(200, 57)
     assert e.value.name == "TooManyShards"
+
+
+@pytest.mark.parametrize("k,m,family,mode,want", [
+    # explicit families: src/core/leopard.rs:225-237 (ceil(k / m') * m' <= order - m', m' = next_pow2(m))
+    (192, 64, "leopard_gf8", "disabled", "leopard_gf8"),
+    (193, 63, "leopard_gf8", "disabled", "TooManyShards"),   # total 256, but 4 x 64 > 256 - 64
+    (200, 100, "leopard_gf8", "disabled", "TooManyShards"),  # total above 256
+    (32768, 16384, "leopard_gf16", "disabled", "leopard_gf16"),
+    (49153, 16383, "leopard_gf16", "disabled", "TooManyShards"),
+    (40000, 30000, "leopard_gf16", "disabled", "TooManyShards"),
+    # automatic selection from Classic: src/core/leopard.rs:191-223
+    (300, 100, "classic", "disabled", "TooManyShards"),
+    (300, 100, "classic", "as_needed", "leopard_gf16"),
+    (200, 56, "classic", "as_needed", "classic"),
+    (10, 4, "classic", "prefer_gf16", "leopard_gf16"),
+    (100, 128, "classic", "prefer_leopard", "leopard_gf8"),
+    (100, 130, "classic", "prefer_leopard", "leopard_gf16"),  # parity above 128
+])
+def test_leopard_family_resolution_and_limits(k, m, family, mode, want):
+    # Family resolution and shape validation run on the host before any
+    # device query: without a GPU an accepted shape reaches the device query
+    # (NoDevice), a rejected one fails first.  With a GPU the resolved family
+    # is read back.
+    import rsgpu
+
+    opts = rsgpu.CodecOptions(codec_family=family, leopard_mode=mode)
+    try:
+        codec = rsgpu.ReedSolomon(k, m, opts)
+    except rsgpu.RsError as e:
+        if e.name == "NoDevice":
+            assert want in ("classic", "leopard_gf8", "leopard_gf16"), (k, m, family, mode)
+            return
+        assert e.name == want, (k, m, family, mode)
+        return
+    assert codec.codec_family() == want, (k, m, family, mode)
