@@ -1,6 +1,5 @@
 """The C-ABI library loads on a CPU-only machine and exports every entry point
 declared in include/rsgpu.h.  No compute call is made here."""
-import ctypes
 import os
 import re
 

@@ -345,8 +345,6 @@ def test_singular_custom_matrix_writes_nothing(rs, torch):
     out0 = torch.full((64,), 0xAB, dtype=torch.uint8, device="cuda")
     out1 = torch.full((64,), 0xAB, dtype=torch.uint8, device="cuda")
     lst = [out0, out1, sh[2], sh[3], sh[4]]
-    import ctypes
-
     mem, ptrs, lens, stream, keep = rs._buffer_info(lst)
     pres = rs._flags([0, 0, 1, 1, 1], 5)
     rc = rs.lib().rsgpu_reconstruct(codec._h, ptrs, lens, pres, 5, 0, rs._flags([], 1), 0, mem, stream)
