@@ -859,6 +859,8 @@ def serving_workload(args, torch, rsgpu, rank, gen):
                               "p99_ms": round(float(np.percentile(lat, 99)), 3),
                               "launches": int(st["launches"]),
                               "host_prepare_frac": round(st["prepare_seconds"] / span, 3),
+                              "max_prepare_ms": round(st["max_prepare_seconds"] * 1e3, 2),
+                              "max_worker_gap_ms": round(st["max_loop_gap_seconds"] * 1e3, 2),
                               "max_concurrent_launches": int(st["max_concurrent_launches"]),
                               "max_reserved_gib": round(st["max_reserved_bytes"] / 2**30, 2)})
     out["budget_gib"] = budget / 2**30

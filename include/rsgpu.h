@@ -484,6 +484,8 @@ typedef struct rsgpu_server_stats {
   size_t pending, inflight, budget_bytes, reserved_bytes, max_reserved_bytes;
   uint32_t max_concurrent_launches, pad;
   double prepare_seconds; /* worker time spent planning, building and launching batches */
+  double max_prepare_seconds;  /* the longest single build-and-launch of a batch */
+  double max_loop_gap_seconds; /* the longest time between two passes of the worker loop */
 } rsgpu_server_stats;
 void rsgpu_server_options_default(rsgpu_server_options *out);
 int32_t rsgpu_server_new(const rsgpu_server_options *opts, rsgpu_server **out);

@@ -225,6 +225,8 @@ class Server {
     s->max_reserved_bytes = max_reserved_;
     s->max_concurrent_launches = max_concurrent_;
     s->prepare_seconds = prepare_s_;
+    s->max_prepare_seconds = max_prepare_s_;
+    s->max_loop_gap_seconds = max_gap_s_;
   }
 
  private:
@@ -241,6 +243,8 @@ class Server {
   size_t inflight_ = 0, reserved_ = 0, max_reserved_ = 0;
   uint32_t max_concurrent_ = 0;
   double prepare_s_ = 0;  // worker time spent building and launching batches
+  double max_prepare_s_ = 0;  // longest single build-and-launch
+  double max_gap_s_ = 0;      // longest time between two passes of the worker loop
   Clock::time_point t0_;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0_).count(); }
@@ -341,6 +345,7 @@ class Server {
         const double dt = sv->now() - t0;
         std::lock_guard<std::mutex> g(sv->mu_);
         sv->prepare_s_ += dt;
+        sv->max_prepare_s_ = std::max(sv->max_prepare_s_, dt);
       }
     } timer{this, t};
     std::vector<size_t> in, out;
@@ -419,13 +424,18 @@ class Server {
 
   void loop() {
     cudaSetDevice(device_);
+    double last = now();
     for (;;) {
+      const double t_pass = now();
+      const double gap = t_pass - last;
+      last = t_pass;
       bool progress = retire();
       for (auto &f : flights_)
         if (!f.busy) progress |= admit_and_launch(f);
       bool idle_exit = false;
       {
         std::unique_lock<std::mutex> g(mu_);
+        max_gap_s_ = std::max(max_gap_s_, gap);
         bool any_busy = false;
         for (auto &f : flights_) any_busy |= f.busy;
         if (stopping_ && pending_.empty() && !any_busy) idle_exit = true;

@@ -129,7 +129,8 @@ class ServerStats(ctypes.Structure):
                 ("pending", ctypes.c_size_t), ("inflight", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t),
                 ("reserved_bytes", ctypes.c_size_t), ("max_reserved_bytes", ctypes.c_size_t),
                 ("max_concurrent_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32),
-                ("prepare_seconds", ctypes.c_double)]
+                ("prepare_seconds", ctypes.c_double), ("max_prepare_seconds", ctypes.c_double),
+                ("max_loop_gap_seconds", ctypes.c_double)]
 
 
 class StreamOptions(ctypes.Structure):
