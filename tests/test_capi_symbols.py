@@ -101,3 +101,68 @@ def test_leopard_family_resolution_and_limits(k, m, family, mode, want):
         assert e.name == want, (k, m, family, mode)
         return
     assert codec.codec_family() == want, (k, m, family, mode)
+
+
+# C struct (include/rsgpu.h) -> its ctypes mirror in the Python package.
+STRUCT_MIRRORS = {
+    "rsgpu_options": "_Options", "rsgpu_cache_stats": "CacheStats", "rsgpu_stream_options": "StreamOptions",
+    "rsgpu_stream_status": "StreamStatus", "rsgpu_mix_op": "MixOp", "rsgpu_plan": "Plan",
+    "rsgpu_mix_options": "MixOptions", "rsgpu_mix_info": "MixInfo", "rsgpu_tune_options": "TuneOptions",
+    "rsgpu_tune_sample": "TuneSample", "rsgpu_train_options": "TrainOptions",
+    "rsgpu_server_options": "ServerOptions", "rsgpu_request": "Request", "rsgpu_completion": "Completion",
+    "rsgpu_server_stats": "ServerStats",
+}
+
+
+def c_members(name):
+    """Member names of `typedef struct name { ... } name;` in the header."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), text, flags=re.S).group(1)
+    out = []
+    for decl in body.split(";"):
+        for i, part in enumerate(decl.split(",")):
+            ids = re.findall(r"[A-Za-z_]\w*", re.sub(r"\[[^\]]*\]", "", part))
+            if ids:
+                out.append(ids[-1])
+    return out
+
+
+def test_every_header_struct_has_a_mirror():
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    assert sorted(re.findall(r"typedef struct (rsgpu_\w+) \{", text)) == sorted(STRUCT_MIRRORS)
+
+
+def test_ctypes_mirrors_match_the_header_layout(tmp_path):
+    # The Python mirror passes these structs by pointer; a size or offset that
+    # differs from the C declaration corrupts memory silently.
+    import shutil
+    import subprocess
+
+    import rsgpu
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    checks, want = [], []
+    for cname, pyname in STRUCT_MIRRORS.items():
+        cls = getattr(rsgpu, pyname)
+        checks.append(f'printf("%zu\\n", sizeof({cname}));')
+        want.append(ctypes_sizeof(cls))
+        members = set(c_members(cname))
+        for field, _ in cls._fields_:
+            if field in members:
+                checks.append(f'printf("%zu\\n", offsetof({cname}, {field}));')
+                want.append(getattr(cls, field).offset)
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "rsgpu.h"\nint main(void) {\n'
+                   + "\n".join(checks) + "\nreturn 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == want, [(c, g, w) for c, g, w in zip(checks, got, want) if g != w]
+
+
+def ctypes_sizeof(cls):
+    import ctypes
+
+    return ctypes.sizeof(cls)
