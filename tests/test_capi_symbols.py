@@ -166,3 +166,24 @@ def ctypes_sizeof(cls):
     import ctypes
 
     return ctypes.sizeof(cls)
+
+
+def header_param_counts():
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for name, params in re.findall(r"\b(rsgpu_\w+)\s*\(([^;{}]*?)\)\s*;", text):
+        params = params.strip()
+        out[name] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_ctypes_signatures_match_the_header_parameter_counts():
+    # The Python mirror binds every entry point the header declares, each
+    # with as many arguments as the header gives it.
+    import rsgpu
+
+    lib = rsgpu.lib()
+    for name, n in header_param_counts().items():
+        argtypes = getattr(lib, name).argtypes
+        assert argtypes is not None, f"{name} is not bound"
+        assert len(argtypes) == n, (name, len(argtypes), n)
