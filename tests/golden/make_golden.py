@@ -154,6 +154,20 @@ def main():
     kats["format_id_gf8_custom_1x1"]["custom_row"] = [0x87]
     kats["format_id_tower_custom_1x1"]["custom_row"] = [[0x12, 0x34]]
 
+    # --- the error enum (src/errors.rs): variants in declaration order (the
+    # C ABI returns discriminant + 1) and each variant's as_str message.
+    rel = "src/errors.rs"
+    t = read(rel)
+    p = t.index("pub enum Error {")
+    body = t[p + len("pub enum Error {"): t.index("}", p)]
+    variants = re.findall(r"^\s*(\w+),", body, flags=re.M)
+    q = t.index("fn as_str(self)")
+    msgs = {}
+    for v in variants:
+        m = re.compile(r"Error::%s\s*=>\s*\{?\s*\"([^\"]*)\"" % v).search(t, q)
+        msgs[v] = m.group(1)
+    kats["error_enum"] = {"where": f"{rel}:{line_of(t, p)}", "variants": variants, "messages": msgs}
+
     with open(OUT, "w") as f:
         json.dump(kats, f, indent=1, sort_keys=True)
     print("wrote", OUT)

@@ -297,3 +297,27 @@ def test_leopard_combo_fit_rejected():
     data = [np.zeros(64, np.uint8) for _ in range(200)]
     rc, _ = O.leopard_encode(8, 200, 50, data)
     assert rc == 2  # TooManyShards
+
+
+def test_error_codes_are_the_reference_discriminants_plus_one(kats):
+    # The C ABI returns the reference Error discriminant + 1 (src/errors.rs),
+    # under the same names in the header and the Python mirror, with the
+    # reference's own message text.
+    import os
+    import re
+
+    import rsgpu
+
+    ref = kats["error_enum"]
+    header = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                               "rsgpu.h")).read()
+    codes = {name: int(v) for name, v in re.findall(r"RSGPU_ERR_(\w+) = (\d+)", header)}
+    assert len(ref["variants"]) == 16
+    for i, variant in enumerate(ref["variants"]):
+        snake = re.sub(r"(?<!^)(?=[A-Z])", "_", variant).upper()
+        assert codes[snake] == i + 1, variant
+        assert rsgpu.ERROR_NAMES[i + 1] == variant
+        assert rsgpu.lib().rsgpu_error_string(i + 1).decode() == ref["messages"][variant], variant
+    # device conditions sit outside the reference's range
+    assert all(v >= 100 for k, v in codes.items() if k not in
+               {re.sub(r"(?<!^)(?=[A-Z])", "_", x).upper() for x in ref["variants"]})
