@@ -168,6 +168,22 @@ def main():
         msgs[v] = m.group(1)
     kats["error_enum"] = {"where": f"{rel}:{line_of(t, p)}", "variants": variants, "messages": msgs}
 
+    # --- CodecOptions::default() (src/core/options.rs): field -> value
+    # (booleans and integers as numbers, enum values by variant name).
+    rel = "src/core/options.rs"
+    t = read(rel)
+    p = t.index("impl Default for CodecOptions")
+    body = t[t.index("Self {", p): t.index("}", t.index("Self {", p))]
+    defaults = {}
+    for name, val in re.findall(r"(\w+):\s*([\w:]+),", body):
+        if val in ("true", "false"):
+            defaults[name] = int(val == "true")
+        elif val.isdigit():
+            defaults[name] = int(val)
+        else:
+            defaults[name] = val.split("::")[-1]
+    kats["codec_options_default"] = {"where": f"{rel}:{line_of(t, p)}", "fields": defaults}
+
     with open(OUT, "w") as f:
         json.dump(kats, f, indent=1, sort_keys=True)
     print("wrote", OUT)

@@ -321,3 +321,26 @@ def test_error_codes_are_the_reference_discriminants_plus_one(kats):
     # device conditions sit outside the reference's range
     assert all(v >= 100 for k, v in codes.items() if k not in
                {re.sub(r"(?<!^)(?=[A-Z])", "_", x).upper() for x in ref["variants"]})
+
+
+def test_default_options_are_the_references(kats):
+    # rsgpu_options_default fills every field the way CodecOptions::default()
+    # does (src/core/options.rs); enum values by the header's names.
+    import os
+    import re
+
+    import rsgpu
+
+    ref = kats["codec_options_default"]["fields"]
+    header = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                               "rsgpu.h")).read()
+    enum = {name: int(v) for name, v in re.findall(r"(RSGPU_\w+) = (\d+)", header)}
+    prefix = {"codec_family": "RSGPU_FAMILY_", "leopard_mode": "RSGPU_LEOPARD_", "matrix_mode": "RSGPU_MATRIX_"}
+    o = rsgpu._Options()
+    rsgpu.lib().rsgpu_options_default(o)
+    assert {f for f, _ in rsgpu._Options._fields_} == set(ref)
+    for field, want in ref.items():
+        got = getattr(o, field)
+        if isinstance(want, str):
+            want = enum[prefix[field] + re.sub(r"(?<!^)(?=[A-Z])", "_", want).upper()]
+        assert got == want, (field, got, want)
