@@ -1,10 +1,12 @@
 """Extract the reference's own known-answer vectors into ``reference_kats.json``.
 
 Run in a checkout that has the reference crate available (default
-``/root/reference``, or ``RS_REFERENCE_ROOT``).  The reference test files are
-read as text only: every literal below is copied out of an assertion in the
-reference test suite, and the file/line of each source is recorded beside it.
-Nothing here executes reference code.
+``/root/reference``, or ``RS_REFERENCE_ROOT``).  The reference files are read
+as text only: the known-answer literals are copied out of assertions in the
+reference test suite, the error enum's variants and messages out of
+src/errors.rs, and CodecOptions::default() out of src/core/options.rs; the
+file/line of each source is recorded beside it.  Nothing here executes
+reference code.
 
     python tests/golden/make_golden.py
 """
