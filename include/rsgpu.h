@@ -5,7 +5,7 @@
  * rustfs-erasure-codec 9.1.0 (a Rust crate with no C ABI of its own).  Every
  * entry point below names the reference API it stands in for (file:line in
  * the reference crate); a Rust binding maps each `ReedSolomon` method onto one
- * call.
+ * call through an `extern "C"` block with these signatures.
  *
  * Conventions
  *  - Return value: 0 on success, otherwise the reference `Error` discriminant
