@@ -171,8 +171,41 @@ int32_t rsgpu_verify_with_workspace(const rsgpu_codec *codec, const uint8_t *con
                                     const size_t *lens, size_t n_shards, rsgpu_verify_ws *ws,
                                     int32_t *ok, int32_t mem, void *stream);
 
+/* src/core/verify.rs:157-176 (verify_with_buffer) and :180-200
+ * (verify_with_buffer_par): the parity recomputed from shards[0..k) is
+ * written into buffer[0..m) (n_buffer == m buffers of the shard length, in
+ * `mem` like the shards) and *ok receives 1 when it equals shards[k..k+m).
+ * Leopard codecs as verify_leopard_with_buffer (src/core/verify.rs:35-57).
+ * Errors: piece count, then TooFew/TooManyBufferShards, then shard sizes. */
+int32_t rsgpu_verify_with_buffer(const rsgpu_codec *codec, const uint8_t *const *shards, const size_t *lens,
+                                 size_t n_shards, uint8_t *const *buffer, const size_t *buffer_lens,
+                                 size_t n_buffer, int32_t *ok, int32_t mem, void *stream);
+
+/* src/galois_8/policy.rs:543-700 (decode_idx): progressive recovery into
+ * caller-initialised destinations.  NULL entries of dst / input stand for
+ * None; both arrays hold k+m entries.  With expect_input (n_expect == k+m
+ * flags), its first k expected indices are the decoding inputs and each call
+ * adds (XOR) into every non-NULL dst the contributions of the inputs it
+ * supplies, so calls over disjoint input batches accumulate the recovered
+ * shards (zero the destinations before the first call).  With expect_input ==
+ * NULL (merge mode), dst[i] ^= input[i] for every supplied input.  The whole
+ * layout is validated before anything is written.  Classic GF(2^8) codecs
+ * only (others: RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY).  dst and input buffers
+ * must not overlap. */
+int32_t rsgpu_decode_idx(const rsgpu_codec *codec, uint8_t *const *dst, const size_t *dst_lens, size_t n_dst,
+                         const uint8_t *expect_input, size_t n_expect, const uint8_t *const *input,
+                         const size_t *input_lens, size_t n_input, int32_t mem, void *stream);
+
 /* src/core/reconstruct.rs:539-726 (prepare_reconstruct_workspace /
- * reconstruct_with_workspace): a reusable plan for one erasure pattern. */
+ * reconstruct_with_workspace): a reusable plan for one erasure pattern.
+ * Classic codecs only, as in the reference (Leopard:
+ * RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY).  Preparing builds (or takes from the
+ * cache) the pattern's decode tables and keeps a private device copy, so a
+ * singular custom matrix fails at prepare time and running the plan does no
+ * cache lookup.  Reuse checks, in order: piece count, family, the codec's
+ * shard counts and encoding format (InvalidCustomMatrix on a different
+ * format), present shard lengths, the same missing pattern
+ * (InvalidShardFlags), the same length (IncorrectShardSize). */
 int32_t rsgpu_prepare_reconstruct_ws(const rsgpu_codec *codec, const uint8_t *present,
                                      size_t n_shards, size_t shard_len, int32_t goal,
                                      const uint8_t *required, size_t n_required,

@@ -449,3 +449,95 @@ int orc_classic_recovery_rows(size_t k, size_t m, const uint8_t *matrix,
   free(p.decode);
   return ORC_OK;
 }
+
+/* src/galois_8/policy.rs:543-700 (decode_idx) with the accumulation of
+ * :79-140 (decode_idx_accumulate_reduced_outputs).  NULL entries of dst /
+ * input stand for None.  With `expect` (n_expect flags), the first k expected
+ * indices select the decoding inputs; each call adds, into every present
+ * destination, the contributions of the inputs supplied in this call:
+ * dst[o] ^= sum_j row_o[j] * input[valid[j]], where row_o is the inverse row
+ * (data o < k) or the parity row times the inverse (parity o >= k) over the
+ * selected columns.  Without `expect` (merge mode), dst[i] ^= input[i] for
+ * every supplied input, after the whole layout has been validated.  The
+ * checks run in the reference's order; an error leaves dst unchanged. */
+int orc_classic_decode_idx(size_t k, size_t m, const uint8_t *matrix, uint8_t *const *dst,
+                           const size_t *dst_lens, size_t n_dst, const uint8_t *expect, size_t n_expect,
+                           const uint8_t *const *input, const size_t *input_lens, size_t n_input) {
+  gf8_init();
+  const size_t total = k + m;
+  /* validate_opt_shard_count over [dst.len(), input.len()] (policy.rs:40-48) */
+  const size_t counts[2] = {n_dst, n_input};
+  for (int i = 0; i < 2; i++) {
+    if (counts[i] < total) return ORC_TOO_FEW_SHARDS;
+    if (counts[i] > total) return ORC_TOO_MANY_SHARDS;
+  }
+  if (!expect) {
+    for (size_t i = 0; i < total; i++) {
+      if (!input[i]) continue;
+      if (!dst[i]) return ORC_TOO_FEW_SHARDS;
+      if (dst_lens[i] != input_lens[i]) return ORC_INCORRECT_SHARD_SIZE;
+    }
+    for (size_t i = 0; i < total; i++)
+      if (input[i])
+        for (size_t b = 0; b < input_lens[i]; b++) dst[i][b] ^= input[i][b];
+    return ORC_OK;
+  }
+  if (n_expect != total) return ORC_INVALID_SHARD_FLAGS;
+  size_t valid[256], n_valid = 0;
+  for (size_t i = 0; i < total; i++)
+    if (expect[i]) valid[n_valid++] = i;
+  if (n_valid < k) return ORC_TOO_FEW_SHARDS_PRESENT;
+  /* shard_len: the first supplied buffer among the inputs, then the destinations */
+  int have_len = 0;
+  size_t len = 0;
+  for (size_t i = 0; i < total && !have_len; i++)
+    if (input[i]) len = input_lens[i], have_len = 1;
+  for (size_t i = 0; i < total && !have_len; i++)
+    if (dst[i]) len = dst_lens[i], have_len = 1;
+  if (!have_len) return ORC_TOO_FEW_SHARDS_PRESENT;
+  for (size_t i = 0; i < total; i++)
+    if (input[i] && input_lens[i] != len) return ORC_INCORRECT_SHARD_SIZE;
+  for (size_t i = 0; i < total; i++)
+    if (dst[i] && dst_lens[i] != len) return ORC_INCORRECT_SHARD_SIZE;
+  size_t outs[256], n_out = 0;
+  for (size_t i = 0; i < total; i++)
+    if (dst[i]) outs[n_out++] = i;
+  if (n_out == 0) return ORC_OK;
+  size_t pos[256], n_pos = 0;
+  for (size_t c = 0; c < k; c++)
+    if (input[valid[c]]) pos[n_pos++] = c;
+  if (n_pos == 0) return ORC_OK;
+  /* get_data_decode_matrix (src/core/reconstruct.rs:1176-1183) wants exactly k selected inputs */
+  if (n_valid != k) return ORC_TOO_FEW_SHARDS_PRESENT;
+  uint8_t *sel = (uint8_t *)malloc(k * k), *dec = (uint8_t *)malloc(k * k);
+  for (size_t r = 0; r < k; r++) memcpy(sel + r * k, matrix + valid[r] * k, k);
+  int rc = orc_gf8_invert(k, sel, dec);
+  free(sel);
+  if (rc != ORC_OK) {
+    free(dec);
+    return ORC_INVALID_CUSTOM_MATRIX;
+  }
+  if (len) {
+    uint8_t *rows = (uint8_t *)malloc(n_out * n_pos);
+    for (size_t o = 0; o < n_out; o++) {
+      const size_t idx = outs[o];
+      for (size_t j = 0; j < n_pos; j++) {
+        const size_t col = pos[j];
+        uint8_t v = 0;
+        if (idx < k) {
+          v = dec[idx * k + col];
+        } else {
+          const uint8_t *prow = matrix + idx * k;
+          for (size_t i = 0; i < k; i++) v ^= MUL8[prow[i]][dec[i * k + col]];
+        }
+        rows[o * n_pos + j] = v;
+      }
+    }
+    for (size_t o = 0; o < n_out; o++)
+      for (size_t j = 0; j < n_pos; j++)
+        orc_gf8_mul_slice_xor(rows[o * n_pos + j], input[valid[pos[j]]], dst[outs[o]], len);
+    free(rows);
+  }
+  free(dec);
+  return ORC_OK;
+}

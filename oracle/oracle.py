@@ -53,6 +53,8 @@ def lib() -> ctypes.CDLL:
                 "orc_classic_recovery_rows": (ctypes.c_int, [size_t, size_t, u8p, u8p, ctypes.c_int, u8p, size_t,
                                                              szp, szp, szp, u8p]),
                 "orc_classic_verify": (ctypes.c_int, [size_t, size_t, u8p, ctypes.POINTER(u8p), size_t]),
+                "orc_classic_decode_idx": (ctypes.c_int, [size_t, size_t, u8p, ctypes.POINTER(u8p), szp, size_t, u8p,
+                                                          size_t, ctypes.POINTER(u8p), szp, size_t]),
                 "orc_lgf8_tables": (None, [u8p, u8p, u8p, u8p]),
                 "orc_lgf8_mul_log": (ctypes.c_uint8, [ctypes.c_uint8, ctypes.c_uint8]),
                 "orc_lgf8_encode": (ctypes.c_int, [size_t, size_t, ctypes.POINTER(u8p), ctypes.POINTER(u8p), size_t]),
@@ -190,6 +192,33 @@ def classic_verify(matrix, shards):
     k = matrix.shape[1]
     m = matrix.shape[0] - k
     return bool(lib().orc_classic_verify(k, m, _p8(matrix), _ptrs(shards), shards[0].size))
+
+
+def _opt_ptrs(arrs):
+    """Pointer and length arrays for a list whose None entries stand for Option::None."""
+    ptrs = (u8p * max(1, len(arrs)))()
+    lens = (size_t * max(1, len(arrs)))()
+    for i, a in enumerate(arrs):
+        if a is not None:
+            ptrs[i] = _p8(a)
+            lens[i] = a.size
+    return ptrs, lens
+
+
+def classic_decode_idx(matrix, dst, expect, inputs):
+    """src/galois_8/policy.rs:543-700: accumulate into the non-None entries of
+    dst (uint8 arrays, changed in place); expect=None selects merge mode."""
+    matrix = np.ascontiguousarray(matrix, np.uint8)
+    k = matrix.shape[1]
+    m = matrix.shape[0] - k
+    dp, dl = _opt_ptrs(dst)
+    ip, il = _opt_ptrs(inputs)
+    if expect is None:
+        ex, nex = None, 0
+    else:
+        ex = np.ascontiguousarray(np.array(expect, np.uint8).reshape(-1))
+        ex, nex = (_p8(ex) if ex.size else _p8(np.zeros(1, np.uint8))), ex.size
+    return lib().orc_classic_decode_idx(k, m, _p8(matrix), dp, dl, len(dst), ex, nex, ip, il, len(inputs))
 
 
 # ---------------------------------------------------------------- Leopard

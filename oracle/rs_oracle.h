@@ -75,6 +75,12 @@ int orc_classic_recovery_rows(size_t k, size_t m, const uint8_t *matrix,
                               size_t *n_targets, uint8_t *rows);
 int orc_classic_verify(size_t k, size_t m, const uint8_t *matrix,
                        const uint8_t *const *shards, size_t len);
+/* Progressive recovery (src/galois_8/policy.rs:543-700): NULL entries of dst /
+ * input are None; expect == NULL selects merge mode. */
+int orc_classic_decode_idx(size_t k, size_t m, const uint8_t *matrix, uint8_t *const *dst,
+                           const size_t *dst_lens, size_t n_dst, const uint8_t *expect,
+                           size_t n_expect, const uint8_t *const *input,
+                           const size_t *input_lens, size_t n_input);
 
 /* ---- Leopard GF(2^8) (src/core/leopard_gf8/) ---- */
 void orc_lgf8_tables(uint8_t *log_lut, uint8_t *exp_lut, uint8_t *fft_skew /*255*/,

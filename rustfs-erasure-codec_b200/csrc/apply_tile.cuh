@@ -186,6 +186,9 @@ __device__ __forceinline__ void apply_tile(const uint8_t *const *ptrs, uint32_t 
             if (VERIFY) {
               uint4 e = ld_stream(dst);
               bad |= (e.x != o[r][0]) | (e.y != o[r][1]) | (e.z != o[r][2]) | (e.w != o[r][3]);
+              if (d.verify_store)
+                st_stream(const_cast<uint8_t *>(ptr[n_in + d.n_out + out]) + col[v],
+                          make_uint4(o[r][0], o[r][1], o[r][2], o[r][3]));
             } else if (ACC) {
               const uint4 e = *reinterpret_cast<const uint4 *>(dst);
               st_stream(dst, make_uint4(o[r][0] ^ e.x, o[r][1] ^ e.y, o[r][2] ^ e.z, o[r][3] ^ e.w));
@@ -220,9 +223,10 @@ __device__ __forceinline__ bool apply_column(const uint8_t *const *ptrs, const J
     for (uint32_t r = 0; r < 4 && g * 4 + r < d.n_out; ++r) {
       uint8_t *dst = const_cast<uint8_t *>(ptr[d.n_in + g * 4 + r]) + col;
       const uint8_t b = uint8_t(acc >> (8 * r));
-      if (VERIFY)
+      if (VERIFY) {
         bad |= (*dst != b);
-      else if (ACC)
+        if (d.verify_store) const_cast<uint8_t *>(ptr[d.n_in + d.n_out + g * 4 + r])[col] = b;
+      } else if (ACC)
         *dst ^= b;
       else
         *dst = b;

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <vector>
 
@@ -41,12 +42,25 @@ struct rsgpu_verify_ws {
   size_t shard_len = 0;
 };
 
+// A prepared reconstruction plan (src/core/workspace.rs:70-112): the erasure
+// layout and goal it was prepared for, the preparing codec's shape and
+// encoding-format identity (reuse by another codec is checked against them,
+// src/core/reconstruct.rs:702-726), and for GF(2^8) codecs the plan's
+// survivors with a private device copy of its decode tables, so running it
+// does no cache lookup and no inversion.
 struct rsgpu_reconstruct_ws {
+  size_t k = 0, m = 0;
+  std::vector<uint8_t> format;
   std::vector<uint8_t> present;
   size_t shard_len = 0;
   int goal = 0;
   std::vector<uint8_t> required;
   std::vector<size_t> targets;
+  std::vector<uint16_t> survivors;
+  uint32_t *tbl = nullptr;
+  ~rsgpu_reconstruct_ws() {
+    if (tbl) cudaFree(tbl);  // waits for queued work that may still read it
+  }
 };
 
 namespace rsgpu {
@@ -299,6 +313,54 @@ int run_host(rsgpu_codec *h, Op op, size_t n_stripes, uint8_t *const *host, cons
   return status;
 }
 
+// Host-memory form of a single-stripe call: every non-null host buffer i gets
+// a device copy of lens[i] bytes, copied in when in[i] and back when out[i];
+// `fn` runs on the device pointers (null where the host pointer is null) on
+// the codec's first internal stream, ordered after the caller's stream, and
+// the call returns once the outputs are back in host memory.
+template <class F>
+int run_host_single(rsgpu_codec *h, size_t n, uint8_t *const *host, const size_t *lens, const std::vector<uint8_t> &in,
+                    const std::vector<uint8_t> &out, void *user_stream, F &&fn) {
+  std::lock_guard<std::mutex> g(h->io_mu);
+  int rc = ensure_io(h);
+  if (rc) return rc;
+  cudaStream_t s = h->io[0];
+  cudaEvent_t ev;
+  RS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  RS_CUDA(cudaEventRecord(ev, S(user_stream)));
+  RS_CUDA(cudaStreamWaitEvent(s, ev, 0));
+  cudaEventDestroy(ev);
+  std::vector<size_t> off(n, 0);
+  size_t bytes = 0;
+  for (size_t i = 0; i < n; ++i) {
+    off[i] = bytes;
+    if (host[i]) bytes += round16(lens[i]);
+  }
+  cudaMemPool_t pool = nullptr;
+  if ((rc = staging_pool(h->c.device, &pool))) return rc;
+  uint8_t *stage = nullptr;
+  RS_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&stage), std::max<size_t>(bytes, 16), pool, s));
+  std::vector<uint8_t *> d(n, nullptr);
+  CopyRun up{cudaMemcpyHostToDevice, s};
+  for (size_t i = 0; i < n; ++i) {
+    if (!host[i]) continue;
+    d[i] = stage + off[i];
+    if (in[i] && lens[i] && (rc = up.add(d[i], host[i], lens[i]))) return rc;
+  }
+  if ((rc = up.flush())) return rc;
+  int status = fn(d.data(), s);
+  if (status == RSGPU_OK) {
+    CopyRun down{cudaMemcpyDeviceToHost, s};
+    for (size_t i = 0; i < n; ++i)
+      if (host[i] && out[i] && lens[i] && (rc = down.add(host[i], d[i], lens[i]))) return rc;
+    if ((rc = down.flush())) return rc;
+  }
+  RS_CUDA(cudaFreeAsync(stage, s));
+  RS_CUDA(cudaStreamSynchronize(s));
+  if (status == RSGPU_OK) status = h->c.take_device_status(s);
+  return status;
+}
+
 // Per-call shard validation for reconstruct (src/core/recovery_plan.rs:262-387).
 int check_reconstruct(const Codec &c, const size_t *lens, const uint8_t *present, size_t n, int goal,
                       const uint8_t *required, size_t n_required, size_t *shard_len) {
@@ -480,6 +542,148 @@ int32_t rsgpu_verify_with_workspace(const rsgpu_codec *h, const uint8_t *const *
   return rc;
 }
 
+int32_t rsgpu_verify_with_buffer(const rsgpu_codec *hc, const uint8_t *const *shards, const size_t *lens, size_t n,
+                                 uint8_t *const *buffer, const size_t *blens, size_t nb, int32_t *ok, int32_t mem,
+                                 void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || !shards || !lens || !ok || !buffer || !blens) return RSGPU_ERR_INVALID_ARGUMENT;
+  Codec &c = h->c;
+  const size_t total = c.k + c.m;
+  // check_piece_count!(all), check_piece_count!(parity_buf),
+  // check_slices!(multi => slices, multi => buffer) (src/core/verify.rs:161-163).
+  if (n < total) return RSGPU_ERR_TOO_FEW_SHARDS;
+  if (n > total) return RSGPU_ERR_TOO_MANY_SHARDS;
+  if (nb < c.m) return RSGPU_ERR_TOO_FEW_BUFFER_SHARDS;
+  if (nb > c.m) return RSGPU_ERR_TOO_MANY_BUFFER_SHARDS;
+  size_t len = 0;
+  int rc = c.check_all(lens, n, &len);
+  if (rc) return rc;
+  if (blens[0] == 0) return RSGPU_ERR_EMPTY_SHARD;
+  for (size_t i = 0; i < nb; ++i)
+    if (blens[i] != blens[0]) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  if (blens[0] != len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  if ((rc = check_family_len(c, len))) return rc;
+  // Device pointers: k data, m stored parity, m buffers.
+  auto run = [&](uint8_t *const *d, cudaStream_t s) -> int {
+    uint8_t flag = 0;
+    int r;
+    if (c.family == RSGPU_FAMILY_CLASSIC && c.field == RSGPU_FIELD_GF8) {
+      r = c.verify_with_buffer_dev(d, len, &flag, s);  // one K1 pass: compare and store
+    } else {
+      // Leopard and the tower field: encode into the buffers, then compare
+      // them with the stored parity (src/core/verify.rs:35-57).
+      std::vector<uint8_t *> enc(d, d + c.k);
+      enc.insert(enc.end(), d + total, d + total + c.m);
+      r = do_encode(c, 1, enc.data(), len, s);
+      std::vector<rsgpu::PairOp> pairs(c.m);
+      for (size_t i = 0; i < c.m; ++i) pairs[i] = {d[total + i], d[c.k + i], len};
+      if (r == RSGPU_OK) r = rsgpu::run_pairs(pairs, rsgpu::PAIR_COMPARE, &flag, s);
+    }
+    if (r == RSGPU_OK) *ok = flag;
+    return r;
+  };
+  std::vector<uint8_t *> all(total + c.m);
+  for (size_t i = 0; i < total; ++i) all[i] = const_cast<uint8_t *>(shards[i]);
+  for (size_t i = 0; i < c.m; ++i) all[total + i] = buffer[i];
+  if (mem == RSGPU_MEM_DEVICE) return run(all.data(), S(stream));
+  std::vector<uint8_t> in(total + c.m, 0), out(total + c.m, 0);
+  std::vector<size_t> hl(total + c.m, len);
+  for (size_t i = 0; i < total; ++i) in[i] = 1;
+  for (size_t i = total; i < total + c.m; ++i) out[i] = 1;
+  return run_host_single(h, total + c.m, all.data(), hl.data(), in, out, stream, run);
+}
+
+int32_t rsgpu_decode_idx(const rsgpu_codec *hc, uint8_t *const *dst, const size_t *dst_lens, size_t n_dst,
+                         const uint8_t *expect, size_t n_expect, const uint8_t *const *input,
+                         const size_t *input_lens, size_t n_input, int32_t mem, void *stream) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || (!dst && n_dst) || (!dst_lens && n_dst) || (!input && n_input) || (!input_lens && n_input))
+    return RSGPU_ERR_INVALID_ARGUMENT;
+  Codec &c = h->c;
+  const size_t total = c.k + c.m;
+  // src/galois_8/policy.rs:543-700, checks in the reference's order.
+  if (c.family != RSGPU_FAMILY_CLASSIC || c.field != RSGPU_FIELD_GF8) return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY;
+  for (size_t cnt : {n_dst, n_input}) {
+    if (cnt < total) return RSGPU_ERR_TOO_FEW_SHARDS;
+    if (cnt > total) return RSGPU_ERR_TOO_MANY_SHARDS;
+  }
+  std::vector<uint8_t> in(2 * total, 0), out(2 * total, 0);
+  std::vector<size_t> hl(2 * total, 0);
+  std::vector<uint8_t *> host(2 * total, nullptr);  // dst[0..total), input[total..2 total)
+  for (size_t i = 0; i < total; ++i) {
+    host[i] = dst[i];
+    hl[i] = dst[i] ? dst_lens[i] : 0;
+    in[i] = out[i] = dst[i] != nullptr;
+    host[total + i] = const_cast<uint8_t *>(input[i]);
+    hl[total + i] = input[i] ? input_lens[i] : 0;
+    in[total + i] = input[i] != nullptr;
+  }
+  std::function<int(uint8_t *const *, cudaStream_t)> run;
+  if (!expect) {
+    // Merge mode: validate every pair, then dst[i] ^= input[i].
+    for (size_t i = 0; i < total; ++i) {
+      if (!input[i]) continue;
+      if (!dst[i]) return RSGPU_ERR_TOO_FEW_SHARDS;
+      if (dst_lens[i] != input_lens[i]) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+    }
+    for (size_t i = 0; i < total; ++i)  // only destinations that receive an input are staged
+      if (!input[i]) host[i] = nullptr, in[i] = out[i] = 0;
+    run = [&](uint8_t *const *d, cudaStream_t s) {
+      std::vector<rsgpu::PairOp> pairs;
+      for (size_t i = 0; i < total; ++i)
+        if (d[total + i] && input_lens[i]) pairs.push_back({d[total + i], d[i], input_lens[i]});
+      return rsgpu::run_pairs(pairs, rsgpu::PAIR_XOR, nullptr, s);
+    };
+  } else {
+    if (n_expect != total) return RSGPU_ERR_INVALID_SHARD_FLAGS;
+    std::vector<uint16_t> valid;
+    for (size_t i = 0; i < total; ++i)
+      if (expect[i]) valid.push_back(uint16_t(i));
+    if (valid.size() < c.k) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+    bool have = false;
+    size_t len = 0;
+    for (size_t i = 0; i < total && !have; ++i)
+      if (input[i]) len = input_lens[i], have = true;
+    for (size_t i = 0; i < total && !have; ++i)
+      if (dst[i]) len = dst_lens[i], have = true;
+    if (!have) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+    for (size_t i = 0; i < total; ++i)
+      if (input[i] && input_lens[i] != len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+    for (size_t i = 0; i < total; ++i)
+      if (dst[i] && dst_lens[i] != len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+    std::vector<uint16_t> outs, cols;
+    for (size_t i = 0; i < total; ++i)
+      if (dst[i]) outs.push_back(uint16_t(i));
+    if (outs.empty()) return RSGPU_OK;
+    for (size_t j = 0; j < c.k; ++j)
+      if (input[valid[j]]) cols.push_back(uint16_t(j));
+    if (cols.empty()) return RSGPU_OK;
+    // get_data_decode_matrix takes exactly k selected inputs
+    // (src/core/reconstruct.rs:1176-1183).
+    if (valid.size() != c.k) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
+    if (len == 0) return RSGPU_OK;
+    run = [&c, valid, outs, cols, len, total](uint8_t *const *d, cudaStream_t s) {
+      return c.decode_idx_dev(valid, outs, cols, d, d + total, len, s);
+    };
+    // Only the inputs that take part are staged.
+    for (size_t i = 0; i < total; ++i) in[total + i] = 0, host[total + i] = nullptr;
+    for (uint16_t j : cols) {
+      const size_t i = valid[j];
+      host[total + i] = const_cast<uint8_t *>(input[i]);
+      in[total + i] = 1;
+    }
+  }
+  if (mem == RSGPU_MEM_DEVICE) {
+    std::vector<uint8_t *> d(2 * total, nullptr);
+    for (size_t i = 0; i < total; ++i) {
+      d[i] = dst[i];
+      d[total + i] = const_cast<uint8_t *>(input[i]);
+    }
+    return run(d.data(), S(stream));
+  }
+  return run_host_single(h, 2 * total, host.data(), hl.data(), in, out, stream, run);
+}
+
 int32_t rsgpu_reconstruct(const rsgpu_codec *hc, uint8_t *const *shards, const size_t *lens, const uint8_t *present,
                           size_t n, int32_t goal, const uint8_t *required, size_t n_required, int32_t mem,
                           void *stream) {
@@ -493,22 +697,37 @@ int32_t rsgpu_reconstruct(const rsgpu_codec *hc, uint8_t *const *shards, const s
   return run_host(h, OP_RECONSTRUCT, 1, shards, present, len, goal, required, n_required, nullptr, stream);
 }
 
-int32_t rsgpu_prepare_reconstruct_ws(const rsgpu_codec *h, const uint8_t *present, size_t n, size_t shard_len,
+int32_t rsgpu_prepare_reconstruct_ws(const rsgpu_codec *hc, const uint8_t *present, size_t n, size_t shard_len,
                                      int32_t goal, const uint8_t *required, size_t n_required,
                                      rsgpu_reconstruct_ws **out) {
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
   if (!h || !present || !out) return RSGPU_ERR_INVALID_ARGUMENT;
-  const Codec &c = h->c;
+  *out = nullptr;
+  Codec &c = h->c;
   const size_t total = c.k + c.m;
+  // prepare_reconstruct_some_workspace checks the mask length first, then
+  // prepare_reconstruct_workspace_with_goal: piece count, family, shard
+  // lengths, then the plan (src/core/reconstruct.rs:586-616,
+  // src/core/recovery_plan.rs:300-326, 413-517).
   if (goal == RSGPU_GOAL_REQUIRED && (!required || (n_required != c.k && n_required != total)))
     return RSGPU_ERR_INVALID_SHARD_FLAGS;
   if (n < total) return RSGPU_ERR_TOO_FEW_SHARDS;
   if (n > total) return RSGPU_ERR_TOO_MANY_SHARDS;
-  if (shard_len == 0) return RSGPU_ERR_EMPTY_SHARD;
+  if (c.family != RSGPU_FAMILY_CLASSIC) return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY;
   size_t np = 0;
   for (size_t i = 0; i < n; ++i) np += present[i] ? 1 : 0;
+  if (np && shard_len == 0) return RSGPU_ERR_EMPTY_SHARD;
   if (np < c.k) return RSGPU_ERR_TOO_FEW_SHARDS_PRESENT;
-  rsgpu_reconstruct_ws *w = new (std::nothrow) rsgpu_reconstruct_ws();
+  int rc = check_family_len(c, shard_len);
+  if (rc) return rc;
+  std::unique_ptr<rsgpu_reconstruct_ws> w(new (std::nothrow) rsgpu_reconstruct_ws());
   if (!w) return RSGPU_ERR_OUT_OF_MEMORY;
+  w->k = c.k;
+  w->m = c.m;
+  size_t flen = 0;
+  if ((rc = rsgpu_format_id(h, nullptr, 0, &flen))) return rc;
+  w->format.resize(flen);
+  if ((rc = rsgpu_format_id(h, w->format.data(), flen, &flen))) return rc;
   w->present.assign(present, present + n);
   w->shard_len = shard_len;
   w->goal = goal;
@@ -519,7 +738,20 @@ int32_t rsgpu_prepare_reconstruct_ws(const rsgpu_codec *h, const uint8_t *presen
              (goal == RSGPU_GOAL_REQUIRED && i < n_required && required[i]);
     if (t) w->targets.push_back(i);
   }
-  *out = w;
+  if (c.field == RSGPU_FIELD_GF8 && !w->targets.empty()) {
+    // The plan's decode tables, built (K3) or taken from the cache now and
+    // copied into memory the workspace owns: a singular custom matrix fails
+    // here, like the reference's eager inverse.
+    rsgpu::ClassicPlan p;
+    if ((rc = c.plan_classic(present, goal, required, n_required, p))) return rc;
+    std::vector<const rsgpu::ClassicPlan *> pp{&p};
+    std::vector<const uint32_t *> tbls;
+    std::lock_guard<std::mutex> g(h->io_mu);
+    if ((rc = ensure_io(h))) return rc;
+    if ((rc = c.decode_tables_copy(pp, tbls, &w->tbl, h->io[0]))) return rc;
+    w->survivors = p.survivors;
+  }
+  *out = w.release();
   return RSGPU_OK;
 }
 
@@ -531,19 +763,66 @@ size_t rsgpu_reconstruct_ws_targets(const rsgpu_reconstruct_ws *ws, size_t *out,
   return ws->targets.size();
 }
 
-int32_t rsgpu_reconstruct_with_ws(const rsgpu_codec *h, rsgpu_reconstruct_ws *ws, uint8_t *const *shards,
+int32_t rsgpu_reconstruct_with_ws(const rsgpu_codec *hc, rsgpu_reconstruct_ws *ws, uint8_t *const *shards,
                                   const size_t *lens, const uint8_t *present, size_t n, int32_t mem, void *stream) {
-  if (!h || !ws || !present || !lens) return RSGPU_ERR_INVALID_ARGUMENT;
-  // Reuse requires the same pattern and length (src/core/recovery_plan.rs:389-413).
-  if (n != ws->present.size()) return n < ws->present.size() ? RSGPU_ERR_TOO_FEW_SHARDS : RSGPU_ERR_TOO_MANY_SHARDS;
+  rsgpu_codec *h = const_cast<rsgpu_codec *>(hc);
+  if (!h || !ws || !present || !lens || !shards) return RSGPU_ERR_INVALID_ARGUMENT;
+  Codec &c = h->c;
+  const size_t total = c.k + c.m;
+  // validate_reconstruct_workspace (src/core/reconstruct.rs:702-726): piece
+  // count, family, the workspace's shape and format, then the layout
+  // (src/core/recovery_plan.rs:390-411): present lengths, the same missing
+  // pattern, the same length.
+  if (n < total) return RSGPU_ERR_TOO_FEW_SHARDS;
+  if (n > total) return RSGPU_ERR_TOO_MANY_SHARDS;
+  if (c.family != RSGPU_FAMILY_CLASSIC) return RSGPU_ERR_UNSUPPORTED_CODEC_FAMILY;
+  if (ws->k < c.k) return RSGPU_ERR_TOO_FEW_DATA_SHARDS;
+  if (ws->k > c.k) return RSGPU_ERR_TOO_MANY_DATA_SHARDS;
+  if (ws->m < c.m) return RSGPU_ERR_TOO_FEW_PARITY_SHARDS;
+  if (ws->m > c.m) return RSGPU_ERR_TOO_MANY_PARITY_SHARDS;
+  size_t flen = 0;
+  int rc = rsgpu_format_id(h, nullptr, 0, &flen);
+  if (rc) return rc;
+  std::vector<uint8_t> fmt(flen);
+  if ((rc = rsgpu_format_id(h, fmt.data(), flen, &flen))) return rc;
+  if (fmt != ws->format) return RSGPU_ERR_INVALID_CUSTOM_MATRIX;
+  size_t len = 0;
+  bool same = true;
   for (size_t i = 0; i < n; ++i) {
-    if (present[i] && lens[i] == 0) return RSGPU_ERR_EMPTY_SHARD;
-    if (present[i] && lens[i] != ws->shard_len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+    if (present[i]) {
+      if (lens[i] == 0) return RSGPU_ERR_EMPTY_SHARD;
+      if (len && lens[i] != len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+      len = lens[i];
+    }
+    same &= (present[i] != 0) == (ws->present[i] != 0);
   }
-  for (size_t i = 0; i < n; ++i)
-    if ((present[i] != 0) != (ws->present[i] != 0)) return RSGPU_ERR_INVALID_SHARD_FLAGS;
-  return rsgpu_reconstruct(h, shards, lens, present, n, ws->goal, ws->required.empty() ? nullptr : ws->required.data(),
-                           ws->required.size(), mem, stream);
+  if (!same) return RSGPU_ERR_INVALID_SHARD_FLAGS;
+  if (len != ws->shard_len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  for (size_t t : ws->targets)
+    if (lens[t] < len) return RSGPU_ERR_INCORRECT_SHARD_SIZE;
+  if (ws->targets.empty()) return RSGPU_OK;
+  if (!ws->tbl)  // tower field: the per-call path over the same plan
+    return rsgpu_reconstruct(h, shards, lens, present, n, ws->goal,
+                             ws->required.empty() ? nullptr : ws->required.data(), ws->required.size(), mem, stream);
+  // GF(2^8): one K1 job over the plan's survivors and targets with the
+  // workspace's own tables.
+  auto run = [&](uint8_t *const *d, cudaStream_t s) {
+    std::vector<rsgpu::JobDesc> jobs(1);
+    jobs[0].n_in = uint16_t(c.k);
+    jobs[0].n_out = uint16_t(ws->targets.size());
+    jobs[0].tbl = ws->tbl;
+    std::vector<const uint8_t *> ptrs;
+    for (uint16_t sv : ws->survivors) ptrs.push_back(d[sv]);
+    for (size_t t : ws->targets) ptrs.push_back(d[t]);
+    return c.apply_jobs(jobs, ptrs, len, s);
+  };
+  if (mem == RSGPU_MEM_DEVICE) return run(shards, S(stream));
+  std::vector<uint8_t> in(n, 0), out(n, 0);
+  std::vector<uint8_t *> host(n, nullptr);
+  std::vector<size_t> hl(n, len);
+  for (uint16_t sv : ws->survivors) host[sv] = shards[sv], in[sv] = 1;
+  for (size_t t : ws->targets) host[t] = shards[t], out[t] = 1;
+  return run_host_single(h, n, host.data(), hl.data(), in, out, stream, run);
 }
 
 int32_t rsgpu_encode_batch(const rsgpu_codec *hc, size_t n_stripes, uint8_t *const *ptrs, size_t len, int32_t mem,

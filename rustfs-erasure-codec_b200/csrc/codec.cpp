@@ -390,7 +390,8 @@ int ApplyLaunch::build(std::vector<JobDesc> &jobs, const std::vector<const uint8
   for (auto &j : jobs) {
     tbl_stage |= j.tbl != jobs[0].tbl;
     bool aligned = true;
-    for (uint32_t i = 0; i < uint32_t(j.n_in) + j.n_out; ++i)
+    const uint32_t n_ptr = uint32_t(j.n_in) + j.n_out * (j.verify_store ? 2u : 1u);
+    for (uint32_t i = 0; i < n_ptr; ++i)
       aligned &= (reinterpret_cast<uintptr_t>(ptrs[j.ptr_off + i]) & 15) == 0;
     j.vec_len = aligned ? (len & ~uint64_t(15)) : 0;
     max_tail = std::max<uint64_t>(max_tail, len - j.vec_len);
@@ -532,6 +533,96 @@ int Codec::verify_dev_async(size_t n_stripes, uint8_t *const *shards, size_t len
   std::vector<const uint8_t *> ptrs;
   encode_jobs(n_stripes, shards, jobs, ptrs, true);
   return run_apply(jobs, ptrs, len, true, flags_dev, s);
+}
+
+int Codec::verify_with_buffer_dev(uint8_t *const *ptrs3, size_t len, uint8_t *ok_host, cudaStream_t s) {
+  std::vector<JobDesc> jobs(1);
+  jobs[0].ptr_off = 0;
+  jobs[0].n_in = uint16_t(k);
+  jobs[0].n_out = uint16_t(m);
+  jobs[0].verify_store = 1;
+  jobs[0].tbl = d_enc_tbl;
+  std::vector<const uint8_t *> ptrs(ptrs3, ptrs3 + k + 2 * m);
+  uint32_t *flags = nullptr;
+  RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&flags), 4, s)));
+  RS_CUDA(cudaMemsetAsync(flags, 0, 4, s));
+  int rc = run_apply(jobs, ptrs, len, true, flags, s);
+  if (rc) return rc;
+  uint32_t f = 0;
+  RS_CUDA(cudaMemcpyAsync(&f, flags, 4, cudaMemcpyDeviceToHost, s));
+  RS_CUDA(cudaFreeAsync(flags, s));
+  if ((rc = take_device_status(s))) return rc;  // also waits for s
+  *ok_host = f ? 0 : 1;
+  return RSGPU_OK;
+}
+
+int run_pairs(const std::vector<PairOp> &pairs, int mode, uint8_t *ok_host, cudaStream_t s) {
+  if (pairs.empty()) {
+    if (ok_host) *ok_host = 1;
+    return RSGPU_OK;
+  }
+  uint64_t max_len = 0;
+  for (const PairOp &p : pairs) max_len = std::max<uint64_t>(max_len, p.len);
+  void *d_pairs = nullptr;
+  int rc = upload(pairs.data(), pairs.size() * sizeof(PairOp), &d_pairs, s);
+  if (rc) return rc;
+  uint32_t *flag = nullptr;
+  if (ok_host) {
+    RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&flag), 4, s)));
+    RS_CUDA(cudaMemsetAsync(flag, 0, 4, s));
+  }
+  RS_CUDA(launch_pairs(static_cast<const PairOp *>(d_pairs), uint32_t(pairs.size()), max_len, mode, flag, s));
+  RS_CUDA(cudaFreeAsync(d_pairs, s));
+  if (ok_host) {
+    uint32_t f = 0;
+    RS_CUDA(cudaMemcpyAsync(&f, flag, 4, cudaMemcpyDeviceToHost, s));
+    RS_CUDA(cudaFreeAsync(flag, s));
+    RS_CUDA(cudaStreamSynchronize(s));
+    *ok_host = f ? 0 : 1;
+  }
+  return RSGPU_OK;
+}
+
+int Codec::decode_idx_dev(const std::vector<uint16_t> &selected, const std::vector<uint16_t> &outs,
+                          const std::vector<uint16_t> &cols, uint8_t *const *dst, const uint8_t *const *input,
+                          size_t len, cudaStream_t s) {
+  ClassicPlan p;
+  p.survivors = selected;
+  p.targets = outs;
+  for (uint16_t o : outs) p.n_data_targets += o < k ? 1 : 0;
+  // The inverse is the identity when the selected inputs are the data shards in order.
+  for (size_t i = 0; i < k; ++i) p.needs_inverse |= selected[i] != i;
+  std::vector<const ClassicPlan *> pp{&p};
+  std::vector<const uint32_t *> tbls;
+  int rc;
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    rc = decode_tables(pp, tbls, s);
+  }
+  if (rc) return rc;
+  const uint32_t groups = uint32_t((outs.size() + 3) / 4);
+  const uint32_t *tbl = tbls[0];
+  uint32_t *reduced = nullptr;
+  if (cols.size() != k) {
+    // Only some of the selected inputs arrive in this call: gather their
+    // columns of the composed rows into a table of their own.
+    GatherCols gc{};
+    for (size_t j = 0; j < cols.size(); ++j) gc.cols[j] = uint8_t(cols[j]);
+    RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&reduced),
+                                         size_t(groups) * cols.size() * kTableWords * 4, s)));
+    RS_CUDA(launch_gather_tables(tbl, reduced, gc, groups, uint32_t(k), uint32_t(cols.size()), s));
+    tbl = reduced;
+  }
+  std::vector<JobDesc> jobs(1);
+  jobs[0].n_in = uint16_t(cols.size());
+  jobs[0].n_out = uint16_t(outs.size());
+  jobs[0].tbl = tbl;
+  std::vector<const uint8_t *> ptrs;
+  for (uint16_t c : cols) ptrs.push_back(input[selected[c]]);
+  for (uint16_t o : outs) ptrs.push_back(dst[o]);
+  rc = run_apply(jobs, ptrs, len, false, nullptr, s, true);
+  if (reduced) RS_CUDA(cudaFreeAsync(reduced, s));
+  return rc;
 }
 
 int Codec::reconstruct_jobs(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, int goal,

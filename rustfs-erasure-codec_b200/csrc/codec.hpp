@@ -136,6 +136,18 @@ class Codec {
   int verify_dev_async(size_t n_stripes, uint8_t *const *shards, size_t len, uint32_t *flags_dev, cudaStream_t s);
   int reconstruct_dev(size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
                       int goal, const uint8_t *required, size_t n_required, cudaStream_t s);
+  // verify_with_buffer (src/core/verify.rs:157-176) in one K1 pass: ptrs3
+  // holds k data, m stored parity and m buffer pointers; the recomputed
+  // parity goes to the buffers and *ok_host says whether it matched.
+  int verify_with_buffer_dev(uint8_t *const *ptrs3, size_t len, uint8_t *ok_host, cudaStream_t s);
+  // decode_idx (src/galois_8/policy.rs:543-700) after validation: `selected`
+  // = the first k expected inputs, `outs` = destination indices, `cols` =
+  // positions among `selected` whose input arrived in this call (ascending);
+  // dst[outs[o]] ^= sum_j row_o[cols[j]] * input[selected[cols[j]]], rows
+  // from the decode-table cache (K3), one accumulating K1 launch.
+  int decode_idx_dev(const std::vector<uint16_t> &selected, const std::vector<uint16_t> &outs,
+                     const std::vector<uint16_t> &cols, uint8_t *const *dst, const uint8_t *const *input,
+                     size_t len, cudaStream_t s);
 
   // Incremental parity (src/core/encode.rs:890-930, 1048-1120): for one
   // stripe, parity_r (+)= sum_j c[r][j] * in[j] over the given inputs, where
@@ -192,5 +204,8 @@ class Codec {
 };
 
 int cuda_status(cudaError_t e);
+// Pair kernel over device buffers (kernels.hpp PairOp): PAIR_COMPARE writes
+// *ok_host (waits for s), PAIR_XOR queues b ^= a and returns.
+int run_pairs(const std::vector<PairOp> &pairs, int mode, uint8_t *ok_host, cudaStream_t s);
 
 }  // namespace rsgpu

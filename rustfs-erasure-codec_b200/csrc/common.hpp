@@ -18,13 +18,15 @@ constexpr uint64_t kApplyTile = uint64_t(kApplyThreads) * kApplyVec;
 // Pointers live in a shared pointer table: ptrs[ptr_off .. ptr_off+n_in) are
 // the inputs and the next n_out entries the outputs (or, for verify, the
 // stored parity to compare against).  Coefficients are pre-packed "nibble
-// tables" (see pack_tables()).
+// tables" (see pack_tables()).  A verify job with verify_store set also
+// writes the recomputed outputs to the n_out pointers that follow the stored
+// parity (verify_with_buffer).
 struct JobDesc {
   uint32_t ptr_off;
   uint16_t n_in;
   uint16_t n_out;
   uint32_t flag_idx;    // verify: index of this stripe's mismatch flag
-  uint32_t reserved;
+  uint32_t verify_store;
   uint64_t vec_len;     // prefix handled by the 128-bit path (0 when misaligned)
   const uint32_t *tbl;  // packed nibble tables of this stripe's coefficient rows
 };

@@ -245,6 +245,9 @@ __global__ void __launch_bounds__(kApplyThreads + 32, 2) k_apply_tma(ApplyArgs a
               if (VERIFY) {
                 const uint4 e = lds128(slot0 + r * kSlot + v * kApplyThreads * kApplyVec);
                 bad |= (e.x != o[r][0]) | (e.y != o[r][1]) | (e.z != o[r][2]) | (e.w != o[r][3]);
+                if (d.verify_store)
+                  st_stream(const_cast<uint8_t *>(a.ptrs[d.ptr_off + n_in + d.n_out + r]) + col[v],
+                            make_uint4(o[r][0], o[r][1], o[r][2], o[r][3]));
               } else {
                 uint8_t *dst = const_cast<uint8_t *>(a.ptrs[d.ptr_off + n_in + r]) + col[v];
                 st_stream(dst, make_uint4(o[r][0], o[r][1], o[r][2], o[r][3]));
@@ -389,6 +392,45 @@ __global__ void __launch_bounds__(256) k_decode_tables(DecodeTableArgs a) {
   if (threadIdx.x == 0) a.status[blockIdx.x] = 0;
 }
 
+// Pair kernel: blockIdx.y selects the pair, the x dimension strides over
+// its 16-byte chunks; pairs whose pointers are not both 16-byte aligned, and
+// the bytes past the last full chunk, go byte by byte.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_pairs(const PairOp *pairs, uint32_t *flag) {
+  const PairOp p = pairs[blockIdx.y];
+  const bool aligned = ((reinterpret_cast<uintptr_t>(p.a) | reinterpret_cast<uintptr_t>(p.b)) & 15) == 0;
+  const uint64_t vec = aligned ? p.len / 16 : 0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  bool bad = false;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < vec; i += stride) {
+    const uint4 x = ld_stream(p.a + 16 * i);
+    if (MODE == PAIR_COMPARE) {
+      const uint4 y = ld_stream(p.b + 16 * i);
+      bad |= (x.x != y.x) | (x.y != y.y) | (x.z != y.z) | (x.w != y.w);
+    } else {
+      uint4 *dst = reinterpret_cast<uint4 *>(p.b + 16 * i);
+      const uint4 y = *dst;
+      st_stream(p.b + 16 * i, make_uint4(x.x ^ y.x, x.y ^ y.y, x.z ^ y.z, x.w ^ y.w));
+    }
+  }
+  for (uint64_t i = 16 * vec + blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < p.len; i += stride) {
+    if (MODE == PAIR_COMPARE)
+      bad |= p.a[i] != p.b[i];
+    else
+      p.b[i] ^= p.a[i];
+  }
+  if (MODE == PAIR_COMPARE && __any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
+__global__ void __launch_bounds__(256) k_gather_tables(const uint32_t *full, uint32_t *out, GatherCols cols,
+                                                       uint32_t groups, uint32_t k_full, uint32_t n_sel) {
+  const uint32_t n = groups * n_sel * kTableWords;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t e = i % kTableWords, j = (i / kTableWords) % n_sel, g = i / (kTableWords * n_sel);
+    out[i] = full[(g * k_full + cols.cols[j]) * kTableWords + e];
+  }
+}
+
 int grid_for(const void *fn, int threads, size_t smem) {
   static int sms = 0;
   if (!sms) {
@@ -477,6 +519,40 @@ cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cud
     ++launches;
   }
   launch_counter_add(launches);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pairs(const PairOp *pairs, uint32_t n, uint64_t max_len, int mode, uint32_t *flag,
+                         cudaStream_t s) {
+  if (n == 0 || max_len == 0) return cudaSuccess;
+  if (n > 65535) return cudaErrorInvalidValue;  // one grid row per pair
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  // About 8 CTAs per SM in total, at least one per 64 KiB of the longest pair.
+  const uint64_t per_pair = (max_len + 65535) / 65536;
+  uint64_t want = (uint64_t(sms) * 8 + n - 1) / n;
+  if (want > per_pair) want = per_pair;
+  if (want < 1) want = 1;
+  const dim3 grid(uint32_t(want), n);
+  if (mode == PAIR_COMPARE)
+    k_pairs<PAIR_COMPARE><<<grid, 256, 0, s>>>(pairs, flag);
+  else
+    k_pairs<PAIR_XOR><<<grid, 256, 0, s>>>(pairs, flag);
+  launch_counter_add(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_tables(const uint32_t *full, uint32_t *out, const GatherCols &cols, uint32_t groups,
+                                 uint32_t k_full, uint32_t n_sel, cudaStream_t s) {
+  const uint32_t n = groups * n_sel * kTableWords;
+  if (n == 0) return cudaSuccess;
+  const uint32_t grid = (n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184;
+  k_gather_tables<<<grid, 256, 0, s>>>(full, out, cols, groups, k_full, n_sel);
+  launch_counter_add(1);
   return cudaGetLastError();
 }
 

@@ -46,4 +46,27 @@ struct DecodeTableArgs {
 };
 cudaError_t launch_decode_tables(const DecodeTableArgs &a, int n_tasks, int max_out, cudaStream_t s);
 
+// Bytewise work over pairs of equally long buffers (device array `pairs`):
+// PAIR_COMPARE ORs 1 into *flag when some pair differs (the comparison step
+// of verify_with_buffer for codecs whose parity comes from a separate encode
+// launch); PAIR_XOR sets b ^= a (decode_idx merge mode).
+struct PairOp {
+  const uint8_t *a;
+  uint8_t *b;
+  uint64_t len;
+};
+enum { PAIR_COMPARE = 0, PAIR_XOR = 1 };
+cudaError_t launch_pairs(const PairOp *pairs, uint32_t n, uint64_t max_len, int mode, uint32_t *flag,
+                         cudaStream_t s);
+
+// Packed tables of a subset of a packed table's input columns: out holds, for
+// every group of 4 outputs, the tables of inputs cols[0..n_sel) of `full`
+// (groups x k_full inputs), in that order (decode_idx over the inputs one
+// call supplies).
+struct GatherCols {
+  uint8_t cols[256];
+};
+cudaError_t launch_gather_tables(const uint32_t *full, uint32_t *out, const GatherCols &cols, uint32_t groups,
+                                 uint32_t k_full, uint32_t n_sel, cudaStream_t s);
+
 }  // namespace rsgpu

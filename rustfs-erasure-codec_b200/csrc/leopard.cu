@@ -1464,6 +1464,9 @@ int na_setup(int dev, NaDevice &d) {
   uint16_t *err = d.err;
   RS_CUDA(cudaMemcpy(const_cast<const uint8_t **>(d.present_ref), &pres, sizeof(pres), cudaMemcpyHostToDevice));
   RS_CUDA(cudaMemcpy(const_cast<uint16_t **>(d.err_ref), &err, sizeof(err), cudaMemcpyHostToDevice));
+  // The GF(2^16) locator needs 128 KiB of dynamic shared memory (raised once
+  // per device here, not at every call).
+  RS_CUDA(ensure_smem_limit(reinterpret_cast<const void *>(k_leo_locator<16>), size_t(1u << 16) * 2));
   (void)dev;
   d.ready = true;
   return RSGPU_OK;
@@ -1511,7 +1514,6 @@ int leopard_reconstruct_noalloc(Codec &c, uint8_t *const *shards, const uint8_t 
     const int bits = st.field->bits;
     const size_t lsmem = size_t(1u << bits) * 2;
     if (bits == 16) {
-      cudaFuncSetAttribute(k_leo_locator<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lsmem));
       k_leo_locator<16><<<1, 1024, lsmem, s>>>(d.present_ref, d.err_ref, st.field->d_walsh, uint32_t(c.k),
                                                uint32_t(c.m), st.m, st.n);
     } else {
@@ -1539,7 +1541,7 @@ int leopard_reconstruct_noalloc(Codec &c, uint8_t *const *shards, const uint8_t 
     // rows of its region), so the scratch needs no clearing between calls.
     const uint64_t tiles = len / 64;
     const uint64_t slots = kNaScratchWords / (uint64_t(st.n) * kRowWords);
-    const int grid = int(std::min<uint64_t>(tiles, std::min<uint64_t>(slots, 4 * 148)));
+    const int grid = int(std::min<uint64_t>(tiles, std::min<uint64_t>(slots, 4 * uint64_t(sm_count()))));
     if (bits == 16)
       k_leo_decode<16, true><<<grid, kLeoThreads, 0, s>>>(a);
     else

@@ -226,6 +226,8 @@ def _lib():
             "rsgpu_verify_ws_new": (I32, [P, SZ, PP]),
             "rsgpu_verify_ws_free": (None, [P]),
             "rsgpu_verify_with_workspace": (I32, [P, PP, SZP, SZ, P, ctypes.POINTER(I32), I32, P]),
+            "rsgpu_verify_with_buffer": (I32, [P, PP, SZP, SZ, PP, SZP, SZ, ctypes.POINTER(I32), I32, P]),
+            "rsgpu_decode_idx": (I32, [P, PP, SZP, SZ, U8P, SZ, PP, SZP, SZ, I32, P]),
             "rsgpu_prepare_reconstruct_ws": (I32, [P, U8P, SZ, SZ, I32, U8P, SZ, PP]),
             "rsgpu_reconstruct_ws_free": (None, [P]),
             "rsgpu_reconstruct_ws_targets": (SZ, [P, SZP, SZ]),
@@ -343,6 +345,13 @@ def _buffer_info(shards):
     return mem, ptrs, lens, stream, keep
 
 
+def _slice_ptrs(ptrs, lens, start, n):
+    """Pointer and length arrays of entries start .. start+n of _buffer_info's arrays."""
+    p = (ctypes.c_void_p * max(1, n))(*ptrs[start:start + n])
+    ln = (ctypes.c_size_t * max(1, n))(*lens[start:start + n])
+    return p, ln
+
+
 def _stripe_block(stripes):
     """(mem, ptr array, shard length, stream, keepalive) when `stripes` is one
     C-contiguous (stripes, shards, length) uint8 block -- a numpy array or a
@@ -431,6 +440,8 @@ class ReconstructWorkspace:
 
     def __init__(self, h):
         self._h = h
+        self.goal = "all"
+        self.required = None
 
     def targets(self) -> List[int]:
         n = _lib().rsgpu_reconstruct_ws_targets(self._h, None, 0)
@@ -930,10 +941,39 @@ class ReedSolomon:
                                                   stream))
         return bool(ok.value)
 
+    def verify_with_buffer(self, shards: Sequence, buffer: Sequence) -> bool:
+        """src/core/verify.rs:157-176: the recomputed parity is left in `buffer`
+        (m buffers of the shard length, host or device like the shards)."""
+        shards, buffer = list(shards), list(buffer)
+        mem, ptrs, lens, stream, keep = _buffer_info(shards + buffer)
+        n = len(shards)
+        ok = ctypes.c_int32(0)
+        sp, sl = _slice_ptrs(ptrs, lens, 0, n)
+        bp, bl = _slice_ptrs(ptrs, lens, n, len(buffer))
+        _check(_lib().rsgpu_verify_with_buffer(self._h, sp, sl, n, bp, bl, len(buffer), ctypes.byref(ok), mem,
+                                               stream))
+        return bool(ok.value)
+
+    # ---------------------------------------------------------- progressive recovery
+    def decode_idx(self, dst: List, expect_input: Optional[Sequence[bool]], inputs: Sequence) -> None:
+        """src/galois_8/policy.rs:543-700: XOR-accumulate into the non-None
+        entries of `dst` (changed in place) the contributions of the non-None
+        entries of `inputs`; expect_input=None merges partial results."""
+        dst, inputs = list(dst), list(inputs)
+        mem, ptrs, lens, stream, keep = _buffer_info(dst + inputs)
+        nd = len(dst)
+        dp, dl = _slice_ptrs(ptrs, lens, 0, nd)
+        ip, il = _slice_ptrs(ptrs, lens, nd, len(inputs))
+        if expect_input is None:
+            ex, nex = None, 0
+        else:
+            ex, nex = _flags(expect_input, max(1, len(expect_input))), len(expect_input)
+        _check(_lib().rsgpu_decode_idx(self._h, dp, dl, nd, ex, nex, ip, il, len(inputs), mem, stream))
+
     # ---------------------------------------------------------- reconstruct
-    def _reconstruct(self, shards: List, goal: str, required=None):
-        # Option<Vec<u8>> semantics: None entries are missing; they receive a
-        # freshly allocated buffer when they are recovery targets.
+    def _fill_targets(self, shards: List, goal: str, required=None) -> List:
+        """Option<Vec<u8>> semantics: None entries are missing; they receive a
+        freshly allocated buffer when they are recovery targets."""
         present = [s is not None for s in shards]
         filled = list(shards)
         known = [s for s in shards if s is not None]
@@ -953,6 +993,11 @@ class ReedSolomon:
                     filled[i] = torch.empty_like(proto)
                 else:
                     filled[i] = np.zeros_like(proto)
+        return filled
+
+    def _reconstruct(self, shards: List, goal: str, required=None):
+        present = [s is not None for s in shards]
+        filled = self._fill_targets(shards, goal, required)
         mem, ptrs, lens, stream, keep = _buffer_info(filled)
         pres = _flags(present, len(shards))
         req = _flags(required or [], max(1, len(required or [])))
@@ -975,19 +1020,40 @@ class ReedSolomon:
 
     def prepare_reconstruct_workspace(self, present: Sequence[bool], shard_len: int, goal: str = "all",
                                       required=None) -> ReconstructWorkspace:
-        """src/core/reconstruct.rs:539-630."""
+        """src/core/reconstruct.rs:539-616: a plan for the erasure layout
+        `present` (one flag per shard) at `shard_len` bytes."""
         h = ctypes.c_void_p()
         req = list(required or [])
-        _check(_lib().rsgpu_prepare_reconstruct_ws(self._h, _flags(present, len(present)), len(present), shard_len,
-                                                   GOAL[goal], _flags(req, max(1, len(req))), len(req),
+        _check(_lib().rsgpu_prepare_reconstruct_ws(self._h, _flags(present, max(1, len(present))), len(present),
+                                                   shard_len, GOAL[goal], _flags(req, max(1, len(req))), len(req),
                                                    ctypes.byref(h)))
-        return ReconstructWorkspace(h)
+        ws = ReconstructWorkspace(h)
+        ws.goal, ws.required = goal, (list(required) if required is not None else None)
+        return ws
 
-    def reconstruct_with_workspace(self, shards: List, present: Sequence[bool], ws: ReconstructWorkspace) -> None:
-        """src/core/reconstruct.rs:631-667: shards must all be buffers; missing ones are outputs."""
-        mem, ptrs, lens, stream, keep = _buffer_info(list(shards))
-        _check(_lib().rsgpu_reconstruct_with_ws(self._h, ws._h, ptrs, lens, _flags(present, len(present)),
-                                                len(shards), mem, stream))
+    def prepare_reconstruct_data_workspace(self, present: Sequence[bool], shard_len: int) -> ReconstructWorkspace:
+        """src/core/reconstruct.rs:546-555."""
+        return self.prepare_reconstruct_workspace(present, shard_len, "data")
+
+    def prepare_reconstruct_some_workspace(self, present: Sequence[bool], shard_len: int,
+                                           required: Sequence[bool]) -> ReconstructWorkspace:
+        """src/core/reconstruct.rs:557-590."""
+        return self.prepare_reconstruct_workspace(present, shard_len, "required", list(required))
+
+    def reconstruct_with_workspace(self, shards: List, ws: ReconstructWorkspace, present=None) -> None:
+        """src/core/reconstruct.rs:618-640.  None entries are missing and
+        receive new buffers when the plan targets them; with `present`, every
+        entry is a buffer and the missing ones are outputs (ShardSlot)."""
+        if present is None:
+            present = [s is not None for s in shards]
+            filled = self._fill_targets(shards, ws.goal, ws.required)
+        else:
+            filled = list(shards)
+        mem, ptrs, lens, stream, keep = _buffer_info(filled)
+        _check(_lib().rsgpu_reconstruct_with_ws(self._h, ws._h, ptrs, lens, _flags(present, max(1, len(present))),
+                                                len(filled), mem, stream))
+        for i in range(len(shards)):
+            shards[i] = filled[i]
 
     # ---------------------------------------------------------- batched
     def encode_batch(self, stripes: Sequence[Sequence]) -> None:

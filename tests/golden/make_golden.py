@@ -1,14 +1,14 @@
 """Extract the reference's own known-answer vectors into ``reference_kats.json``.
 
-Run in a checkout that has the reference crate available (default
-``/root/reference``, or ``RS_REFERENCE_ROOT``).  The reference files are read
+Run with ``RS_REFERENCE_ROOT`` set to the root of a checkout of the
+reference crate (rustfs-erasure-codec 9.1.0).  The reference files are read
 as text only: the known-answer literals are copied out of assertions in the
 reference test suite, the error enum's variants and messages out of
 src/errors.rs, and CodecOptions::default() out of src/core/options.rs; the
 file/line of each source is recorded beside it.  Nothing here executes
 reference code.
 
-    python tests/golden/make_golden.py
+    RS_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -16,7 +16,7 @@ import json
 import os
 import re
 
-REF = os.environ.get("RS_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("RS_REFERENCE_ROOT", "")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 
@@ -49,6 +49,8 @@ def bracket_after(text, start):
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        raise SystemExit("set RS_REFERENCE_ROOT to the root of a reference crate checkout")
     kats = {"source": "rustfs-erasure-codec 9.1.0 test suite (literal assertions)"}
 
     # --- GF(2^8) field (src/galois_8/tests.rs)

@@ -347,3 +347,32 @@ def test_tower_gf16_classic(rs, torch):
         lst = [None if i in lost else sh[i] for i in range(k + m)]
         c.reconstruct(lst)
         assert all(np.array_equal(lst[i].cpu().numpy(), ref[i]) for i in range(k + m))
+
+
+@pytest.mark.parametrize("goal", ["all", "data"])
+def test_tower_gf16_reconstruct_non_codeword(rs, torch, goal):
+    # Random shards that are not a codeword: the rebuilt shards must follow the
+    # reference's survivor rule and row algebra, not merely round-trip.
+    for k, m, size in [(4, 2, 64), (10, 4, 2 * 2049), (20, 10, 1000)]:
+        rc, mat = O.gf16t_build_matrix(k, m)
+        c = rs.ReedSolomon(k, m, field="gf16")
+        rng = np.random.default_rng(k * 3 + m + len(goal))
+        for _ in range(4):
+            shards = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k + m)]
+            e = int(rng.integers(1, m + 1))
+            lost = set(rng.choice(k + m, size=e, replace=False).tolist())
+            pres = [0 if i in lost else 1 for i in range(k + m)]
+            ref = [s.copy() for s in shards]
+            assert O.gf16t_reconstruct(mat, ref, pres, data_only=(goal == "data")) == 0
+            lst = [None if i in lost else torch.from_numpy(shards[i].copy()).cuda() for i in range(k + m)]
+            if goal == "all":
+                c.reconstruct(lst)
+            else:
+                c.reconstruct_data(lst)
+            for i in range(k + m):
+                if i in lost and (goal == "all" or i < k):
+                    assert np.array_equal(lst[i].cpu().numpy(), ref[i]), (k, m, goal, sorted(lost), i)
+                elif i not in lost:
+                    assert np.array_equal(lst[i].cpu().numpy(), shards[i])
+                else:
+                    assert lst[i] is None
