@@ -238,6 +238,8 @@ int Codec::decode_tables(const std::vector<const ClassicPlan *> &plans, std::vec
   for (size_t i = 0; i < plans.size(); ++i) {
     const ClassicPlan &p = *plans[i];
     if (p.all_present || p.targets.empty()) continue;
+    // A table block holds the rows of at most m outputs over k inputs.
+    if (p.targets.size() > m || p.survivors.size() != k) return RSGPU_ERR_INVALID_ARGUMENT;
     PatternKey key = key_of(p, k);
     ++stats_.requests;
     if (use_cache) {
@@ -586,13 +588,21 @@ int run_pairs(const std::vector<PairOp> &pairs, int mode, uint8_t *ok_host, cuda
 int Codec::decode_idx_dev(const std::vector<uint16_t> &selected, const std::vector<uint16_t> &outs,
                           const std::vector<uint16_t> &cols, uint8_t *const *dst, const uint8_t *const *input,
                           size_t len, cudaStream_t s) {
-  ClassicPlan p;
-  p.survivors = selected;
-  p.targets = outs;
-  for (uint16_t o : outs) p.n_data_targets += o < k ? 1 : 0;
-  // The inverse is the identity when the selected inputs are the data shards in order.
-  for (size_t i = 0; i < k; ++i) p.needs_inverse |= selected[i] != i;
-  std::vector<const ClassicPlan *> pp{&p};
+  // A decode-table block holds the packed rows of at most m outputs, so the
+  // destinations go in chunks of m, one table and one K1 job per chunk.
+  bool identity = true;  // the selected inputs are the data shards in order
+  for (size_t i = 0; i < k; ++i) identity &= selected[i] == i;
+  std::vector<ClassicPlan> plans;
+  for (size_t o0 = 0; o0 < outs.size(); o0 += m) {
+    ClassicPlan p;
+    p.survivors = selected;
+    p.targets.assign(outs.begin() + o0, outs.begin() + std::min(outs.size(), o0 + m));
+    for (uint16_t o : p.targets) p.n_data_targets += o < k ? 1 : 0;
+    p.needs_inverse = !identity;
+    plans.push_back(std::move(p));
+  }
+  std::vector<const ClassicPlan *> pp;
+  for (const ClassicPlan &p : plans) pp.push_back(&p);
   std::vector<const uint32_t *> tbls;
   int rc;
   {
@@ -600,26 +610,35 @@ int Codec::decode_idx_dev(const std::vector<uint16_t> &selected, const std::vect
     rc = decode_tables(pp, tbls, s);
   }
   if (rc) return rc;
-  const uint32_t groups = uint32_t((outs.size() + 3) / 4);
-  const uint32_t *tbl = tbls[0];
+  const size_t n_sel = cols.size();
+  // Only some of the selected inputs arrive in this call: gather their
+  // columns of each chunk's rows into tables of their own.
   uint32_t *reduced = nullptr;
-  if (cols.size() != k) {
-    // Only some of the selected inputs arrive in this call: gather their
-    // columns of the composed rows into a table of their own.
+  std::vector<size_t> red_off(plans.size(), 0);
+  if (n_sel != k) {
+    size_t words = 0;
+    for (size_t c = 0; c < plans.size(); ++c) {
+      red_off[c] = words;
+      words += packed_table_words(plans[c].targets.size(), n_sel);
+    }
+    RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&reduced), words * 4, s)));
     GatherCols gc{};
-    for (size_t j = 0; j < cols.size(); ++j) gc.cols[j] = uint8_t(cols[j]);
-    RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&reduced),
-                                         size_t(groups) * cols.size() * kTableWords * 4, s)));
-    RS_CUDA(launch_gather_tables(tbl, reduced, gc, groups, uint32_t(k), uint32_t(cols.size()), s));
-    tbl = reduced;
+    for (size_t j = 0; j < n_sel; ++j) gc.cols[j] = uint8_t(cols[j]);
+    for (size_t c = 0; c < plans.size(); ++c) {
+      const uint32_t groups = uint32_t((plans[c].targets.size() + 3) / 4);
+      RS_CUDA(launch_gather_tables(tbls[c], reduced + red_off[c], gc, groups, uint32_t(k), uint32_t(n_sel), s));
+    }
   }
-  std::vector<JobDesc> jobs(1);
-  jobs[0].n_in = uint16_t(cols.size());
-  jobs[0].n_out = uint16_t(outs.size());
-  jobs[0].tbl = tbl;
+  std::vector<JobDesc> jobs(plans.size());
   std::vector<const uint8_t *> ptrs;
-  for (uint16_t c : cols) ptrs.push_back(input[selected[c]]);
-  for (uint16_t o : outs) ptrs.push_back(dst[o]);
+  for (size_t c = 0; c < plans.size(); ++c) {
+    jobs[c].ptr_off = uint32_t(ptrs.size());
+    jobs[c].n_in = uint16_t(n_sel);
+    jobs[c].n_out = uint16_t(plans[c].targets.size());
+    jobs[c].tbl = reduced ? reduced + red_off[c] : tbls[c];
+    for (uint16_t col : cols) ptrs.push_back(input[selected[col]]);
+    for (uint16_t o : plans[c].targets) ptrs.push_back(dst[o]);
+  }
   rc = run_apply(jobs, ptrs, len, false, nullptr, s, true);
   if (reduced) RS_CUDA(cudaFreeAsync(reduced, s));
   return rc;

@@ -144,7 +144,8 @@ class Codec {
   // = the first k expected inputs, `outs` = destination indices, `cols` =
   // positions among `selected` whose input arrived in this call (ascending);
   // dst[outs[o]] ^= sum_j row_o[cols[j]] * input[selected[cols[j]]], rows
-  // from the decode-table cache (K3), one accumulating K1 launch.
+  // from the decode-table cache (K3, one entry per m destinations), one
+  // accumulating K1 launch.
   int decode_idx_dev(const std::vector<uint16_t> &selected, const std::vector<uint16_t> &outs,
                      const std::vector<uint16_t> &cols, uint8_t *const *dst, const uint8_t *const *input,
                      size_t len, cudaStream_t s);
