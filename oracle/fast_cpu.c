@@ -8,10 +8,12 @@
  * once per group of up to four outputs, with the output sums held in
  * registers) using GF2P8AFFINEQB when the host has GFNI
  * (src/galois_8/x86/gfni.rs:121-215, matrices derived as in
- * src/galois_8/mod.rs:9-33), and the split-nibble PSHUFB formulation of
- * src/galois_8/x86/avx2.rs:85-155 otherwise.  Stripes are spread over
- * threads the way the reference's rayon jobs spread chunks
- * (src/core/encode.rs:1177-1265).
+ * src/galois_8/mod.rs:9-33), at 64-byte width when the host also has
+ * AVX-512 (the reference's first choice, src/galois_8/backend.rs:396-413,
+ * dot_avx512 in gfni_rows.rs) and at 32-byte width otherwise, and the
+ * split-nibble PSHUFB formulation of src/galois_8/x86/avx2.rs:85-155 without
+ * GFNI.  Stripes are spread over threads the way the reference's rayon jobs
+ * spread chunks (src/core/encode.rs:1177-1265).
  */
 #include <immintrin.h>
 #include <pthread.h>
@@ -25,8 +27,13 @@ static int have_gfni(void) {
   return __builtin_cpu_supports("gfni") && __builtin_cpu_supports("avx2");
 }
 
+static int have_gfni512(void) {
+  __builtin_cpu_init();
+  return have_gfni() && __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw");
+}
+
 const char *orc_fast_kernel_name(void) {
-  return have_gfni() ? "gfni-avx2-rows" : "avx2-nibble-rows";
+  return have_gfni512() ? "gfni-avx512-rows" : have_gfni() ? "gfni-avx2-rows" : "avx2-nibble-rows";
 }
 
 static uint64_t gfni_matrix(uint8_t c) {
@@ -43,7 +50,7 @@ typedef struct {
   size_t k, m, len, n_stripes, next_stripe_stride, first;
   const uint8_t *matrix;
   uint8_t *const *ptrs;
-  int gfni;
+  int gfni;      /* 2: GFNI at 64-byte width, 1: at 32-byte width, 0: nibble tables */
   size_t chunk;  /* columns per job: work is spread over (stripe, column chunk) */
 } job_t;
 
@@ -65,6 +72,35 @@ __attribute__((target("avx2,gfni"))) static void rows_gfni(const job_t *j, uint8
           acc[o] = _mm256_xor_si256(acc[o], _mm256_gf2p8affine_epi64_epi8(v, mats[o][i], 0));
       }
       for (size_t o = 0; o < no; o++) _mm256_storeu_si256((__m256i *)(sh[k + g + o] + x), acc[o]);
+    }
+    for (; x < len; x++)
+      for (size_t o = 0; o < no; o++) {
+        uint8_t a = 0;
+        for (size_t i = 0; i < k; i++) a ^= orc_gf8_mul(j->matrix[(k + g + o) * k + i], sh[i][x]);
+        sh[k + g + o][x] = a;
+      }
+  }
+}
+
+__attribute__((target("avx512f,avx512bw,gfni"))) static void rows_gfni512(const job_t *j, uint8_t *const *sh,
+                                                                            size_t x0, size_t len) {
+  size_t k = j->k, m = j->m;
+  for (size_t g = 0; g < m; g += 4) {
+    size_t no = m - g < 4 ? m - g : 4;
+    __m512i mats[4][256];
+    for (size_t o = 0; o < no; o++)
+      for (size_t i = 0; i < k; i++)
+        mats[o][i] = _mm512_set1_epi64((long long)gfni_matrix(j->matrix[(k + g + o) * k + i]));
+    size_t x = x0;
+    for (; x + 64 <= len; x += 64) {
+      __m512i acc[4] = {_mm512_setzero_si512(), _mm512_setzero_si512(), _mm512_setzero_si512(),
+                        _mm512_setzero_si512()};
+      for (size_t i = 0; i < k; i++) {
+        __m512i v = _mm512_loadu_si512((const void *)(sh[i] + x));
+        for (size_t o = 0; o < no; o++)
+          acc[o] = _mm512_xor_si512(acc[o], _mm512_gf2p8affine_epi64_epi8(v, mats[o][i], 0));
+      }
+      for (size_t o = 0; o < no; o++) _mm512_storeu_si512((void *)(sh[k + g + o] + x), acc[o]);
     }
     for (; x < len; x++)
       for (size_t o = 0; o < no; o++) {
@@ -123,7 +159,9 @@ static void *worker(void *arg) {
     size_t s = q / per, c = q % per;
     size_t x0 = c * j->chunk, x1 = x0 + j->chunk < j->len ? x0 + j->chunk : j->len;
     uint8_t *const *sh = j->ptrs + s * (j->k + j->m);
-    if (j->gfni)
+    if (j->gfni == 2)
+      rows_gfni512(j, sh, x0, x1);
+    else if (j->gfni)
       rows_gfni(j, sh, x0, x1);
     else
       rows_nibble(j, sh, x0, x1);
@@ -134,7 +172,7 @@ static void *worker(void *arg) {
 int orc_fast_encode_batch(size_t k, size_t m, const uint8_t *matrix, uint8_t *const *shard_ptrs,
                           size_t n_stripes, size_t len, int threads) {
   if (k > 256 || threads < 1) return ORC_TOO_MANY_SHARDS;
-  int gfni = have_gfni();
+  int gfni = have_gfni512() ? 2 : have_gfni();
   pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)threads);
   job_t *jobs = (job_t *)malloc(sizeof(job_t) * (size_t)threads);
   for (int t = 0; t < threads; t++) {

@@ -344,3 +344,22 @@ def test_default_options_are_the_references(kats):
         if isinstance(want, str):
             want = enum[prefix[field] + re.sub(r"(?<!^)(?=[A-Z])", "_", want).upper()]
         assert got == want, (field, got, want)
+
+
+def test_timed_cpu_row_kernel_matches_the_oracle_encode():
+    # The benchmark's CPU baseline (GFNI rows at the host's widest vector, or
+    # nibble tables) must compute the same parity as the scalar restatement,
+    # including shard lengths with a ragged tail and recovery-row matrices.
+    for k, m, size, n in [(10, 4, 4096 + 37, 3), (16, 4, 1000, 2), (4, 2, 70, 5), (20, 10, 999, 2)]:
+        rc, mat = O.build_matrix(k, m)
+        rng = np.random.default_rng(k + m + size)
+        flat = []
+        for _ in range(n):
+            flat += [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)]
+            flat += [np.zeros(size, np.uint8) for _ in range(m)]
+        assert O.fast_encode_batch(mat, flat, n, size, 3) == 0
+        for s in range(n):
+            ref = [a.copy() for a in flat[s * (k + m): s * (k + m) + k]] + [np.zeros(size, np.uint8) for _ in range(m)]
+            O.classic_encode(mat, ref)
+            for i in range(k + m):
+                assert (ref[i] == flat[s * (k + m) + i]).all(), (k, m, s, i, O.fast_kernel_name())
