@@ -32,8 +32,23 @@ static int have_gfni512(void) {
   return have_gfni() && __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw");
 }
 
+/* -1: the reference's own choice (widest GFNI the host has); otherwise a
+ * forced kernel (2: GFNI at 64 bytes, 1: GFNI at 32 bytes, 0: nibble tables),
+ * clamped to what the host supports. */
+static int forced_kernel = -1;
+
+static int selected_kernel(void) {
+  const int best = have_gfni512() ? 2 : have_gfni() ? 1 : 0;
+  return forced_kernel < 0 || forced_kernel > best ? best : forced_kernel;
+}
+
+void orc_fast_force_kernel(int kernel) { forced_kernel = kernel; }
+
+int orc_fast_best_kernel(void) { return have_gfni512() ? 2 : have_gfni() ? 1 : 0; }
+
 const char *orc_fast_kernel_name(void) {
-  return have_gfni512() ? "gfni-avx512-rows" : have_gfni() ? "gfni-avx2-rows" : "avx2-nibble-rows";
+  const int k = selected_kernel();
+  return k == 2 ? "gfni-avx512-rows" : k == 1 ? "gfni-avx2-rows" : "avx2-nibble-rows";
 }
 
 static uint64_t gfni_matrix(uint8_t c) {
@@ -172,7 +187,7 @@ static void *worker(void *arg) {
 int orc_fast_encode_batch(size_t k, size_t m, const uint8_t *matrix, uint8_t *const *shard_ptrs,
                           size_t n_stripes, size_t len, int threads) {
   if (k > 256 || threads < 1) return ORC_TOO_MANY_SHARDS;
-  int gfni = have_gfni512() ? 2 : have_gfni();
+  int gfni = selected_kernel();
   pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)threads);
   job_t *jobs = (job_t *)malloc(sizeof(job_t) * (size_t)threads);
   for (int t = 0; t < threads; t++) {

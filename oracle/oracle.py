@@ -73,6 +73,8 @@ def lib() -> ctypes.CDLL:
                 "orc_fast_encode_batch": (ctypes.c_int, [size_t, size_t, u8p, ctypes.POINTER(u8p), size_t, size_t,
                                                          ctypes.c_int]),
                 "orc_fast_kernel_name": (ctypes.c_char_p, []),
+                "orc_fast_force_kernel": (None, [ctypes.c_int]),
+                "orc_fast_best_kernel": (ctypes.c_int, []),
             }
             for name, (res, args) in sig.items():
                 fn = getattr(L, name)
@@ -299,6 +301,16 @@ def fast_encode_batch(matrix, shard_arrays, n_stripes, length, threads):
 
 def fast_kernel_name():
     return lib().orc_fast_kernel_name().decode()
+
+
+def fast_force_kernel(kernel: int) -> None:
+    """-1: the host's widest GFNI (the reference's choice); 2 / 1: GFNI at 64 /
+    32 bytes; 0: nibble tables."""
+    lib().orc_fast_force_kernel(kernel)
+
+
+def fast_best_kernel() -> int:
+    return int(lib().orc_fast_best_kernel())
 
 
 # ---------------------------------------------------------------- checksums

@@ -119,6 +119,12 @@ int orc_fast_encode_batch(size_t k, size_t m, const uint8_t *matrix,
                           uint8_t *const *shard_ptrs /* n_stripes*(k+m) */,
                           size_t n_stripes, size_t len, int threads);
 const char *orc_fast_kernel_name(void);
+/* Kernel choice of orc_fast_encode_batch: -1 = the host's widest GFNI (the
+ * reference's selection order), 2 / 1 = GFNI at 64 / 32 bytes, 0 = nibble
+ * tables; the best kernel the host supports is reported by
+ * orc_fast_best_kernel. */
+void orc_fast_force_kernel(int kernel);
+int orc_fast_best_kernel(void);
 
 #ifdef __cplusplus
 }

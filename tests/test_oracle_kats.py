@@ -357,9 +357,16 @@ def test_timed_cpu_row_kernel_matches_the_oracle_encode():
         for _ in range(n):
             flat += [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)]
             flat += [np.zeros(size, np.uint8) for _ in range(m)]
-        assert O.fast_encode_batch(mat, flat, n, size, 3) == 0
-        for s in range(n):
-            ref = [a.copy() for a in flat[s * (k + m): s * (k + m) + k]] + [np.zeros(size, np.uint8) for _ in range(m)]
-            O.classic_encode(mat, ref)
-            for i in range(k + m):
-                assert (ref[i] == flat[s * (k + m) + i]).all(), (k, m, s, i, O.fast_kernel_name())
+        for kernel in range(O.fast_best_kernel() + 1):
+            O.fast_force_kernel(kernel)
+            for s in range(n):
+                for r in range(m):
+                    flat[s * (k + m) + k + r][:] = 0xEE
+            assert O.fast_encode_batch(mat, flat, n, size, 3) == 0
+            for s in range(n):
+                ref = [a.copy() for a in flat[s * (k + m): s * (k + m) + k]] + [np.zeros(size, np.uint8)
+                                                                                for _ in range(m)]
+                O.classic_encode(mat, ref)
+                for i in range(k + m):
+                    assert (ref[i] == flat[s * (k + m) + i]).all(), (k, m, s, i, O.fast_kernel_name())
+        O.fast_force_kernel(-1)
