@@ -376,3 +376,29 @@ def test_tower_gf16_reconstruct_non_codeword(rs, torch, goal):
                     assert np.array_equal(lst[i].cpu().numpy(), shards[i])
                 else:
                     assert lst[i] is None
+
+
+@pytest.mark.parametrize("k,m,size", [(1500, 100, 192), (1000, 600, 320), (600, 1000, 64), (1024, 512, 4096)])
+def test_lgf16_2048_lane_decode_shapes(rs, torch, k, m, size):
+    # 2048 transform lanes with shard lengths down to one 64-byte block:
+    # non-codeword inputs, truncated transforms (k + m well below n, few
+    # parity lanes, more parity than data), goals all and data.
+    rng = np.random.default_rng(k * 5 + m + size)
+    full = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k + m)]
+    c = codec(rs, 16, k, m)
+    for e, goal in ((m, "all"), (int(rng.integers(1, m)), "all"), (int(rng.integers(1, m + 1)), "data")):
+        lost = set(rng.choice(k + m, size=e, replace=False).tolist())
+        pres = [0 if i in lost else 1 for i in range(k + m)]
+        ref = [s.copy() for s in full]
+        for i in lost:
+            ref[i][:] = 0
+        want = [1 if (goal == "all" or i < k) else 0 for i in range(k + m)]
+        assert O.leopard_reconstruct(16, k, m, ref, pres, want) == 0
+        buf = torch.from_numpy(np.stack(full)).cuda()
+        lst = [None if i in lost else buf[i] for i in range(k + m)]
+        (c.reconstruct if goal == "all" else c.reconstruct_data)(lst)
+        for i in sorted(lost):
+            if goal == "data" and i >= k:
+                assert lst[i] is None
+            else:
+                assert np.array_equal(lst[i].cpu().numpy(), ref[i]), (k, m, e, goal, i)
