@@ -565,7 +565,10 @@ int32_t rsgpu_leopard_reconstruct_noalloc(const rsgpu_codec *codec, uint8_t *con
 
 /* ------------------------------------------------------------ introspection */
 /* src/core/codec.rs:412-414 (reconstruction_cache_stats): device decode-table
- * cache of this codec. */
+ * cache of a classic codec; for Leopard codecs, the error-locator cache (one
+ * entry per erasure pattern, least recently used patterns evicted beyond
+ * 32 MiB or 64 patterns, whichever is larger; the reference bounds its
+ * decode-plan cache the same way, src/core/leopard_gf16/decode.rs:268-305). */
 int32_t rsgpu_get_cache_stats(const rsgpu_codec *codec, rsgpu_cache_stats *out);
 /* Number of kernels this process launched through the library so far. */
 uint64_t rsgpu_kernel_launch_count(void);

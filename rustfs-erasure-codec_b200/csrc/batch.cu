@@ -288,6 +288,7 @@ struct MixBatch {
   uint32_t *d_flags = nullptr;
   uint32_t *d_counter = nullptr;
   uint32_t *d_scratch = nullptr;
+  uint16_t *d_locs = nullptr;     // the batch's copies of its Leopard error locators
   bool scratch_borrowed = false;  // d_scratch belongs to the caller's ScratchSlot
   MixArgs args{};
   size_t smem = 0;
@@ -307,12 +308,13 @@ struct MixBatch {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (stream_ordered) {
-      for (void *p : {(void *)d_blob, (void *)d_flags, (void *)d_counter})
+      for (void *p : {(void *)d_blob, (void *)d_flags, (void *)d_counter, (void *)d_locs})
         if (p) cudaFreeAsync(p, stream);
       if (d_scratch && !scratch_borrowed) cudaFreeAsync(d_scratch, stream);
       return;
     }
-    if (d_blob || d_flags || d_counter || d_scratch) cudaDeviceSynchronize();
+    if (d_blob || d_flags || d_counter || d_scratch || d_locs) cudaDeviceSynchronize();
+    if (d_locs) cudaFree(d_locs);
     if (d_blob) cudaFree(d_blob);
     if (d_flags) cudaFree(d_flags);
     if (d_counter) cudaFree(d_counter);
@@ -512,15 +514,30 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   // ---- Leopard FFT reconstructions: error locators per codec.
   std::vector<const uint16_t *> lerr(n_ops, nullptr);
   std::vector<uint32_t> lin(n_ops, 0);
+  // The batch keeps its own copies of the locators (one device buffer for
+  // all its patterns), so the codec's cache may evict them meanwhile.
+  size_t loc_words = 0;
+  for (auto &kv : leo_fft_rec) {
+    LeoGeometry g{};
+    int rc = leopard_geometry(const_cast<Codec &>(*kv.first), &g);
+    if (rc) return rc;
+    loc_words += kv.second.size() * size_t(g.n);
+  }
+  if (loc_words) RS_CUDA(b.alloc(&b.d_locs, loc_words * 2));
+  size_t loc_used = 0;
   for (auto &kv : leo_fft_rec) {
     Codec &c = const_cast<Codec &>(*kv.first);
     const size_t total = c.k + c.m;
+    LeoGeometry g{};
+    leopard_geometry(c, &g);
     std::vector<uint8_t> pres(kv.second.size() * total);
     for (size_t x = 0; x < kv.second.size(); ++x) std::memcpy(&pres[x * total], ops[kv.second[x]].present, total);
     std::vector<const uint16_t *> err(kv.second.size());
     std::vector<uint32_t> ic(kv.second.size());
-    int rc = leopard_locators(c, kv.second.size(), pres.data(), err.data(), ic.data(), s);
+    int rc = leopard_locators(c, kv.second.size(), pres.data(), b.d_locs + loc_used, err.data(), ic.data(), s,
+                              b.stream_ordered);
     if (rc) return rc;
+    loc_used += kv.second.size() * size_t(g.n);
     for (size_t x = 0; x < kv.second.size(); ++x) {
       lerr[kv.second[x]] = err[x];
       lin[kv.second[x]] = ic[x];

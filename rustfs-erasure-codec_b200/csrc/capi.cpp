@@ -938,7 +938,11 @@ void rsgpu_batch_free(rsgpu_batch *b) { delete b; }
 
 int32_t rsgpu_get_cache_stats(const rsgpu_codec *h, rsgpu_cache_stats *out) {
   if (!h || !out) return RSGPU_ERR_INVALID_ARGUMENT;
-  const_cast<rsgpu_codec *>(h)->c.stats(out);
+  Codec &c = const_cast<rsgpu_codec *>(h)->c;
+  if (c.family != RSGPU_FAMILY_CLASSIC)
+    rsgpu::leopard_cache_stats(c, out);  // the error-locator cache
+  else
+    c.stats(out);
   return RSGPU_OK;
 }
 

@@ -335,25 +335,58 @@ __global__ void __launch_bounds__(1024) k_leo_locator(const uint8_t *const *pres
 }  // namespace
 
 // ====================================================================== host
+using EventPtr = std::shared_ptr<CUevent_st>;
+
+// A cached error-locator array.  Launches never read it in place: every
+// build copies the locators it needs into memory the launch owns, in stream
+// order, under the cache lock (copy_locators), and records an event after the
+// copies.  A plan evicted from the cache gives its block back only behind
+// those events, so a copy still queued on some stream always reads the
+// pattern it was queued for.
 struct LeoPlan {
-  uint16_t *err = nullptr;  // device, n entries
+  uint16_t *err = nullptr;  // device, n entries (one block of the locator pool)
   uint32_t input_count = 0;
   // Completion of the launch that builds err (null once seen complete):
-  // a launch that uses the plan waits on it in stream order instead of the
+  // a copy that uses the plan waits on it in stream order instead of the
   // builder waiting on the host.
-  std::shared_ptr<CUevent_st> ready;
+  EventPtr ready;
+  // Copies from err that may still be queued (pruned as they complete).
+  std::vector<EventPtr> readers;
+  std::list<std::string>::iterator lru;
+  uint64_t pinned_by = 0;  // the build that last used it cannot evict it
 };
+
+// A block of an evicted plan, reusable once its readers (and its own
+// locator launch) have finished in stream order.
+struct RetiredBlock {
+  uint16_t *err;
+  EventPtr ready;
+  std::vector<EventPtr> readers;
+};
+
+// Locator arrays cached per codec: least recently used patterns beyond this
+// many bytes are evicted (the reference bounds its GF(2^16) decode-plan cache
+// the same way, src/core/leopard_gf16/decode.rs:268-305, 405-445).  At least
+// 64 patterns are kept whatever the code's width.
+constexpr size_t kLocatorCacheBytes = size_t(32) << 20;
+constexpr size_t kLocatorCacheMinPlans = 64;
 
 struct LeopardState {
   LeoField *field = nullptr;
   uint32_t m = 0, n = 0, mtrunc = 0, last = 0;
   std::mutex mu;
   std::unordered_map<std::string, LeoPlan> plans;
+  std::list<std::string> plan_lru;  // least recently used first
+  size_t plan_block = 0;            // bytes of one locator block (2n, 256-aligned)
+  size_t plan_budget = 0;           // bytes the cached plans may hold
+  rsgpu_cache_stats plan_stats{};   // requests, hits, misses, inserts, evictions
+  uint64_t build_seq = 0;           // id of the build in progress (under mu)
   std::vector<void *> owned;    // retired scratch slabs, freed with the codec
-  // Locator arrays of the cached plans are carved from these slabs (plans
-  // live as long as the codec), so a new pattern costs no cudaMalloc.
+  // Locator blocks are carved from these slabs, so a new pattern costs no
+  // cudaMalloc once the pool has grown to the cache's budget.
   std::vector<void *> plan_slabs;
-  size_t slab_used = 0, slab_bytes = 0;
+  std::vector<uint16_t *> free_blocks;
+  std::vector<RetiredBlock> retired_blocks;
   uint32_t *scratch = nullptr;  // global work rows for the decode of very wide codes
   size_t scratch_bytes = 0;
   // Launches that use `scratch` are ordered across streams by this event:
@@ -431,6 +464,8 @@ int Codec::init_leopard() {
   st->n = uint32_t(pow2_at_least(st->m + k));
   st->mtrunc = uint32_t(std::min<size_t>(k, st->m));
   st->last = uint32_t(k % st->m);
+  st->plan_block = (size_t(st->n) * 2 + 255) & ~size_t(255);
+  st->plan_budget = std::max(kLocatorCacheBytes, kLocatorCacheMinPlans * st->plan_block);
   const uint32_t mod = st->field->host.mod;
   if (st->m > mod) return RSGPU_ERR_TOO_MANY_SHARDS;
   leo = st;
@@ -622,36 +657,86 @@ int configure(const K kernel, LeoLaunch &L, uint32_t lanes, size_t len, uint64_t
   return RSGPU_OK;
 }
 
-// Error locators for a presence pattern, built on the GPU (K7a) and kept
-// resident; returns the plan.
+// Makes stream s wait for the events that are still pending (a null or
+// completed event needs no wait).
+int wait_events(const std::vector<EventPtr> &evs, cudaStream_t s) {
+  for (const EventPtr &e : evs)
+    if (e && cudaEventQuery(e.get()) != cudaSuccess) RS_CUDA(cudaStreamWaitEvent(s, e.get(), 0));
+  return RSGPU_OK;
+}
+
+// A locator block for a new plan, its previous users ordered before stream
+// s: a free block, else a retired one (s waits for the copies that read it
+// and for the launch that wrote it), else a new slab's worth.
+int take_block(LeopardState &st, cudaStream_t s, uint16_t **out) {
+  if (st.free_blocks.empty() && !st.retired_blocks.empty()) {
+    RetiredBlock r = std::move(st.retired_blocks.back());
+    st.retired_blocks.pop_back();
+    r.readers.push_back(r.ready);
+    const int rc = wait_events(r.readers, s);
+    if (rc) return rc;
+    *out = r.err;
+    return RSGPU_OK;
+  }
+  if (st.free_blocks.empty()) {
+    const size_t per = std::max<size_t>(1, (size_t(1) << 20) / st.plan_block);
+    void *p = nullptr;
+    RS_CUDA(cudaMalloc(&p, per * st.plan_block));
+    st.plan_slabs.push_back(p);
+    for (size_t i = 0; i < per; ++i)
+      st.free_blocks.push_back(reinterpret_cast<uint16_t *>(static_cast<uint8_t *>(p) + i * st.plan_block));
+  }
+  *out = st.free_blocks.back();
+  st.free_blocks.pop_back();
+  return RSGPU_OK;
+}
+
+// Evicts least recently used plans until one more block fits the budget;
+// plans the current build uses stay (the cache may then run over its budget
+// until a later build).
+void evict_for_one(LeopardState &st) {
+  while ((st.plans.size() + 1) * st.plan_block > st.plan_budget && !st.plan_lru.empty()) {
+    auto it = st.plans.find(st.plan_lru.front());
+    if (it->second.pinned_by == st.build_seq) break;  // every older plan is gone already
+    st.retired_blocks.push_back(RetiredBlock{it->second.err, it->second.ready, std::move(it->second.readers)});
+    st.plan_lru.pop_front();
+    st.plans.erase(it);
+    ++st.plan_stats.evictions;
+  }
+}
+
+// Error locators for a presence pattern, built on the GPU (K7a) and cached
+// (least recently used out beyond the budget); returns the plan, pinned for
+// the current build.  Caller holds st.mu and has started a build
+// (st.build_seq).
 int decode_plan(Codec &c, const uint8_t *present, LeoPlan **out, cudaStream_t s,
                 std::vector<std::pair<std::string, const uint8_t *>> &pending) {
   LeopardState &st = *c.leo;
   std::string key(reinterpret_cast<const char *>(present), c.k + c.m);
+  ++st.plan_stats.requests;
   auto it = st.plans.find(key);
   if (it != st.plans.end()) {
+    ++st.plan_stats.hits;
+    st.plan_lru.splice(st.plan_lru.end(), st.plan_lru, it->second.lru);
+    it->second.pinned_by = st.build_seq;
     *out = &it->second;
     return RSGPU_OK;
   }
+  ++st.plan_stats.misses;
+  evict_for_one(st);
   LeoPlan plan;
-  const size_t bytes = (size_t(st.n) * 2 + 255) & ~size_t(255);
-  if (st.plan_slabs.empty() || st.slab_used + bytes > st.slab_bytes) {
-    const size_t sz = std::max<size_t>(size_t(1) << 20, bytes);
-    void *p = nullptr;
-    RS_CUDA(cudaMalloc(&p, sz));
-    st.plan_slabs.push_back(p);
-    st.slab_used = 0;
-    st.slab_bytes = sz;
-  }
-  plan.err = reinterpret_cast<uint16_t *>(static_cast<uint8_t *>(st.plan_slabs.back()) + st.slab_used);
-  st.slab_used += bytes;
+  int rc = take_block(st, s, &plan.err);
+  if (rc) return rc;
   plan.input_count = st.m;
   for (size_t i = 0; i < c.k; ++i)
     if (present[i]) plan.input_count = uint32_t(st.m + i + 1);
-  auto ins = st.plans.emplace(key, plan);
+  plan.pinned_by = st.build_seq;
+  auto ins = st.plans.emplace(key, std::move(plan));
+  st.plan_lru.push_back(key);
+  ins.first->second.lru = std::prev(st.plan_lru.end());
+  ++st.plan_stats.inserts;
   pending.emplace_back(key, present);
   *out = &ins.first->second;
-  (void)s;
   return RSGPU_OK;
 }
 
@@ -723,6 +808,31 @@ int wait_plans(const std::vector<LeoPlan *> &plans, cudaStream_t s) {
   return RSGPU_OK;
 }
 
+// Copies the locators of `plans` (distinct) to dst + i * n on stream s, after
+// their locator launches.  With `ordered` the copies stay queued on s and an
+// event recorded behind them joins each plan's readers (an evicted block is
+// reused only after it); otherwise the call waits for s.  Caller holds st.mu.
+int copy_locators(LeopardState &st, const std::vector<LeoPlan *> &plans, uint16_t *dst, cudaStream_t s,
+                  bool ordered) {
+  if (plans.empty()) return RSGPU_OK;
+  int rc = wait_plans(plans, s);
+  if (rc) return rc;
+  for (size_t i = 0; i < plans.size(); ++i)
+    RS_CUDA(cudaMemcpyAsync(dst + i * st.n, plans[i]->err, size_t(st.n) * 2, cudaMemcpyDeviceToDevice, s));
+  if (!ordered) return cuda_status(cudaStreamSynchronize(s));
+  cudaEvent_t ev = nullptr;
+  RS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  EventPtr read(ev, [](cudaEvent_t e) { cudaEventDestroy(e); });
+  RS_CUDA(cudaEventRecord(ev, s));
+  for (LeoPlan *p : plans) {
+    auto &r = p->readers;
+    r.erase(std::remove_if(r.begin(), r.end(), [](const EventPtr &e) { return cudaEventQuery(e.get()) == cudaSuccess; }),
+            r.end());
+    r.push_back(read);
+  }
+  return RSGPU_OK;
+}
+
 int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
               int goal, const uint8_t *required, size_t n_required, uint32_t *flags, LeoLaunch &L,
               cudaStream_t s, bool one_shot) {
@@ -735,9 +845,14 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
   std::vector<uint8_t> roles;
   std::vector<size_t> role_off;
   {
+    // The lock covers the plans, their locator launches and the copies of the
+    // locators into this launch's blob.
     std::lock_guard<std::mutex> g(st.mu);
+    ++st.build_seq;
     std::vector<std::pair<std::string, const uint8_t *>> pending;
-    std::vector<LeoPlan *> used;
+    std::vector<LeoPlan *> used;       // distinct plans, in first-use order
+    std::vector<uint32_t> slot_of_job;  // index into `used` per decode job
+    std::unordered_map<LeoPlan *, uint32_t> slot;
     int bad = RSGPU_OK;  // an unrecoverable stripe: plans already cached still get their locators
     for (size_t i = 0; i < n_stripes && bad == RSGPU_OK; ++i) {
       LeoJob j{};
@@ -768,39 +883,47 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
         }
         LeoPlan *plan = nullptr;
         if ((bad = decode_plan(c, pr, &plan, s, pending))) break;
-        j.err = plan->err;
+        auto sl = slot.emplace(plan, uint32_t(used.size()));
+        if (sl.second) used.push_back(plan);
+        slot_of_job.push_back(sl.first->second);
         j.input_count = plan->input_count;
-        used.push_back(plan);
         role_off.push_back(base);
       }
       jobs.push_back(j);
     }
-    int rc = build_locators(c, pending, s);
-    if (!rc) rc = wait_plans(used, s);
+    int rc = build_locators(c, pending, s);  // plans already cached get their locators even on an error
     if (rc) return rc;
     if (bad) return bad;
+    // Blob: jobs | pointers | roles | locators (one array per distinct pattern).
+    const size_t jb = jobs.size() * sizeof(LeoJob);
+    const size_t pb = n_stripes * total * sizeof(void *);
+    const size_t lo = (jb + pb + roles.size() + 255) & ~size_t(255);
+    const size_t lb = used.size() * size_t(st.n) * 2;
+    std::vector<uint8_t> blob(lo);
+    std::memcpy(blob.data() + jb, shards, pb);
+    std::memcpy(blob.data() + jb + pb, roles.data(), roles.size());
+    if (one_shot) {
+      RS_CUDA(cudaError_t(lib_malloc_async(&L.d_blob, lo + lb + 16, s)));
+      L.blob_ordered = true;
+      L.blob_stream = s;
+    } else {
+      RS_CUDA(cudaMalloc(&L.d_blob, lo + lb + 16));
+    }
+    uint8_t *dbase = static_cast<uint8_t *>(L.d_blob);
+    uint16_t *locs = reinterpret_cast<uint16_t *>(dbase + lo);
+    for (size_t i = 0; i < jobs.size() && L.decode; ++i) {
+      jobs[i].role = dbase + jb + pb + role_off[i];
+      jobs[i].err = locs + size_t(slot_of_job[i]) * st.n;
+    }
+    std::memcpy(blob.data(), jobs.data(), jb);
+    if (one_shot)
+      RS_CUDA(cudaMemcpyAsync(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, s));
+    else
+      RS_CUDA(cudaMemcpy(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+    if ((rc = copy_locators(st, used, locs, s, one_shot))) return rc;
   }
-  // Blob: jobs | pointers | roles.
   const size_t jb = jobs.size() * sizeof(LeoJob);
-  const size_t pb = n_stripes * total * sizeof(void *);
-  std::vector<uint8_t> blob(jb + pb + roles.size() + 16);
-  std::memcpy(blob.data() + jb, shards, pb);
-  std::memcpy(blob.data() + jb + pb, roles.data(), roles.size());
-  if (one_shot) {
-    RS_CUDA(cudaError_t(lib_malloc_async(&L.d_blob, std::max<size_t>(blob.size(), 16), s)));
-    L.blob_ordered = true;
-    L.blob_stream = s;
-  } else {
-    RS_CUDA(cudaMalloc(&L.d_blob, std::max<size_t>(blob.size(), 16)));
-  }
   uint8_t *dbase = static_cast<uint8_t *>(L.d_blob);
-  for (size_t i = 0; i < jobs.size(); ++i)
-    if (L.decode) jobs[i].role = dbase + jb + pb + role_off[i];
-  std::memcpy(blob.data(), jobs.data(), jb);
-  if (one_shot)
-    RS_CUDA(cudaMemcpyAsync(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, s));
-  else
-    RS_CUDA(cudaMemcpy(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
   LeoArgs &a = L.args;
   a.jobs = reinterpret_cast<const LeoJob *>(dbase);
   a.ptrs = reinterpret_cast<const uint8_t *const *>(dbase + jb);
@@ -1202,25 +1325,40 @@ int leopard_geometry(Codec &c, LeoGeometry *g) {
   return RSGPU_OK;
 }
 
-int leopard_locators(Codec &c, size_t n, const uint8_t *present, const uint16_t **err, uint32_t *input_count,
-                     cudaStream_t s) {
+int leopard_locators(Codec &c, size_t n, const uint8_t *present, uint16_t *dst, const uint16_t **err,
+                     uint32_t *input_count, cudaStream_t s, bool ordered) {
   LeopardState &st = *c.leo;
   const size_t total = c.k + c.m;
   std::lock_guard<std::mutex> g(st.mu);
+  ++st.build_seq;
   std::vector<std::pair<std::string, const uint8_t *>> pending;
-  std::vector<LeoPlan *> plans(n, nullptr);
+  std::vector<LeoPlan *> used;
+  std::unordered_map<LeoPlan *, uint32_t> slot;
+  std::vector<uint32_t> slot_of(n, 0);
   int bad = RSGPU_OK;
-  for (size_t i = 0; i < n && bad == RSGPU_OK; ++i) bad = decode_plan(c, present + i * total, &plans[i], s, pending);
-  int rc = build_locators(c, pending, s);  // plans already cached get their locators even on an error
-  if (!rc) rc = wait_plans(plans, s);
-  if (!rc) rc = bad;
-  if (rc) return rc;
-  // unordered_map nodes are stable, so the plan pointers are still valid.
-  for (size_t i = 0; i < n; ++i) {
-    err[i] = plans[i]->err;
-    input_count[i] = plans[i]->input_count;
+  for (size_t i = 0; i < n && bad == RSGPU_OK; ++i) {
+    LeoPlan *p = nullptr;
+    bad = decode_plan(c, present + i * total, &p, s, pending);
+    if (bad) break;
+    auto sl = slot.emplace(p, uint32_t(used.size()));
+    if (sl.second) used.push_back(p);
+    slot_of[i] = sl.first->second;
+    input_count[i] = p->input_count;
   }
+  int rc = build_locators(c, pending, s);  // plans already cached get their locators even on an error
+  if (!rc) rc = bad;
+  if (!rc) rc = copy_locators(st, used, dst, s, ordered);
+  if (rc) return rc;
+  for (size_t i = 0; i < n; ++i) err[i] = dst + size_t(slot_of[i]) * st.n;
   return RSGPU_OK;
+}
+
+void leopard_cache_stats(Codec &c, rsgpu_cache_stats *out) {
+  LeopardState &st = *c.leo;
+  std::lock_guard<std::mutex> g(st.mu);
+  *out = st.plan_stats;
+  out->entries = st.plans.size();
+  out->retained_bytes = st.plans.size() * st.plan_block;
 }
 
 const uint8_t (*leopard_mul8())[256] {

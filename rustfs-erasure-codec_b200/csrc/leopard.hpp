@@ -9,6 +9,8 @@
 #include <memory>
 #include <vector>
 
+#include "rsgpu.h"
+
 namespace rsgpu {
 
 class Codec;
@@ -50,9 +52,15 @@ struct LeoGeometry {
 };
 int leopard_geometry(Codec &c, LeoGeometry *g);
 // Error locators of n presence patterns (k + m flags each), built on the GPU
-// for patterns not seen before; the pointers stay valid for the codec's life.
-int leopard_locators(Codec &c, size_t n, const uint8_t *present, const uint16_t **err, uint32_t *input_count,
-                     cudaStream_t s);
+// for patterns not in the codec's cache and copied into the caller's device
+// buffer `dst` (room for n arrays of the geometry's n lanes); err[i] points at
+// pattern i's array there (patterns that repeat share one).  With `ordered`
+// the copies are queued on s; otherwise the call waits for them.
+int leopard_locators(Codec &c, size_t n, const uint8_t *present, uint16_t *dst, const uint16_t **err,
+                     uint32_t *input_count, cudaStream_t s, bool ordered);
+// Statistics of the codec's error-locator cache (entries = cached patterns,
+// retained_bytes = their device bytes).
+void leopard_cache_stats(Codec &c, rsgpu_cache_stats *out);
 // Leopard GF(2^8) products: mul[a][b] in the codec field's representation.
 const uint8_t (*leopard_mul8())[256];
 // The GF(2^8) Leopard encode as a dense m x k matrix over the Leopard field
