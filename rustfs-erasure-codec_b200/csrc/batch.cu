@@ -423,7 +423,7 @@ int add_apply_job(MixBuild &B, const rsgpu_plan &plan, bool verify, size_t n_in,
 }  // namespace
 
 int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, const rsgpu_mix_options &opt,
-              MixPtr &out, cudaStream_t ordered, ScratchSlot *scratch) {
+              MixPtr &out, cudaStream_t ordered, ScratchSlot *scratch, std::vector<DenseWant> *deferred) {
   int device = 0;
   RS_CUDA(cudaGetDevice(&device));
   for (size_t i = 0; i < n_ops; ++i) {
@@ -457,8 +457,14 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
         if (ops[i].op != RSGPU_OP_RECONSTRUCT || c.family != RSGPU_FAMILY_LEOPARD_GF8 ||
             b.plans[i].algo != RSGPU_ALGO_APPLY)
           continue;
-        if (!leopard_dense_due(c, ops[i].present, ops[i].goal, ops[i].shard_len))
+        if (!leopard_dense_due(c, ops[i].present, ops[i].goal, ops[i].shard_len)) {
           b.plans[i] = mix_default_plan(c, ops[i].op, ops[i].shard_len);
+        } else if (deferred && !leopard_dense_cached(c, ops[i].present, ops[i].goal)) {
+          b.plans[i] = mix_default_plan(c, ops[i].op, ops[i].shard_len);
+          deferred->push_back(DenseWant{ops[i].codec,
+                                        std::string(reinterpret_cast<const char *>(ops[i].present), c.k + c.m),
+                                        ops[i].goal});
+        }
       }
     refine_small_batch(ops, n_ops, b.plans);
   }

@@ -6,6 +6,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "rsgpu.h"
@@ -30,13 +31,25 @@ struct ScratchSlot {
   size_t bytes = 0;
 };
 
+// A Leopard GF(2^8) rebuild pattern whose dense map is due but not derived
+// yet (one-shot batches with `deferred` only).
+struct DenseWant {
+  const rsgpu_codec *codec;
+  std::string pattern;  // k + m presence flags
+  int goal;
+};
+
 // Prepare a mixed batch; `forced` (optional) gives every op's plan.
 // With `ordered`, the batch is a one-shot, stream-ordered batch for that
 // stream (no graph): its device memory is allocated and freed in the stream's
 // order and building it never synchronizes the device; `scratch` (optional,
-// one-shot batches) supplies its work rows.
+// one-shot batches) supplies its work rows.  With `deferred` (one-shot
+// batches), a due pattern whose map is not cached runs the FFT decode in this
+// batch and is listed in *deferred, for the caller to derive off the request
+// path; without it the map is derived before the launch.
 int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, const rsgpu_mix_options &opt,
-              MixPtr &out, cudaStream_t ordered = nullptr, ScratchSlot *scratch = nullptr);
+              MixPtr &out, cudaStream_t ordered = nullptr, ScratchSlot *scratch = nullptr,
+              std::vector<DenseWant> *deferred = nullptr);
 // The validation mix_build applies to each operation (reference error
 // precedence; shard pointers must be non-null).
 int mix_validate(const rsgpu_mix_op &o, int device);

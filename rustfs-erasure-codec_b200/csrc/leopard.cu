@@ -1437,12 +1437,15 @@ int leopard_dense_encode(Codec &c, std::vector<uint8_t> &rows) {
 
 namespace {
 
-// Derives the maps of n patterns with one FFT decode over unit-vector
-// stripes: the q-th present shard of pattern i holds the identity element at
-// column q, so target t column q is coefficient (t, q) of that pattern's map.
-int derive_dense8(Codec &c, size_t n, const uint8_t *present, int goal, std::vector<LeoDenseMap> &maps,
-                  cudaStream_t s) {
-  const size_t k = c.k, m = c.m, total = k + m;
+// Maps are derived with one FFT decode over unit-vector stripes: the q-th
+// present shard of pattern i holds the identity element at column q, so
+// target t column q of the decoded stripes is coefficient (t, q) of that
+// pattern's map.  dense_layout fills every map's inputs and targets and
+// returns the column count L (the widest map's inputs, in 64-byte blocks);
+// dense_units writes the unit vectors into a host image of n stripes;
+// dense_extract reads the coefficients back out and packs the K1 tables.
+size_t dense_layout(const Codec &c, size_t n, const uint8_t *present, int goal, std::vector<LeoDenseMap> &maps) {
+  const size_t k = c.k, total = k + c.m;
   maps.assign(n, LeoDenseMap{});
   size_t max_in = 1;
   for (size_t i = 0; i < n; ++i) {
@@ -1456,12 +1459,39 @@ int derive_dense8(Codec &c, size_t n, const uint8_t *present, int goal, std::vec
     }
     max_in = std::max(max_in, mp.inputs.size());
   }
-  const size_t L = (max_in + 63) / 64 * 64;
-  std::vector<uint8_t> host(n * total * L, 0);
+  return (max_in + 63) / 64 * 64;
+}
+
+void dense_units(const Codec &c, const std::vector<LeoDenseMap> &maps, size_t L, uint8_t *host) {
+  const size_t total = c.k + c.m;
+  std::memset(host, 0, maps.size() * total * L);
   const uint8_t one = leo8_one();
-  for (size_t i = 0; i < n; ++i)
+  for (size_t i = 0; i < maps.size(); ++i)
     for (size_t q = 0; q < maps[i].inputs.size(); ++q) host[(i * total + maps[i].inputs[q]) * L + q] = one;
-  // Stream-ordered on `s`; the host waits for `s` only, to read the maps.
+}
+
+void dense_extract(const Codec &c, std::vector<LeoDenseMap> &maps, size_t L, const uint8_t *host) {
+  const size_t total = c.k + c.m;
+  for (size_t i = 0; i < maps.size(); ++i) {
+    LeoDenseMap &mp = maps[i];
+    const size_t ni = mp.inputs.size(), nt = mp.targets.size();
+    mp.rows.assign(nt * ni, 0);
+    for (size_t t = 0; t < nt; ++t)
+      for (size_t q = 0; q < ni; ++q) mp.rows[t * ni + q] = host[(i * total + mp.targets[t]) * L + q];
+    auto packed = std::make_shared<std::vector<uint32_t>>(packed_table_words(nt, ni));
+    pack_tables_with(leopard_mul8(), mp.rows.data(), nt, ni, packed->data());
+    mp.packed = std::move(packed);
+  }
+}
+
+// Derives the maps of n patterns (one FFT decode, stream-ordered on s; the
+// host waits for s only, to read the maps back).
+int derive_dense8(Codec &c, size_t n, const uint8_t *present, int goal, std::vector<LeoDenseMap> &maps,
+                  cudaStream_t s) {
+  const size_t total = c.k + c.m;
+  const size_t L = dense_layout(c, n, present, goal, maps);
+  std::vector<uint8_t> host(n * total * L, 0);
+  dense_units(c, maps, L, host.data());
   uint8_t *d = nullptr;
   RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&d), host.size(), s)));
   int rc = cuda_status(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, s));
@@ -1472,17 +1502,29 @@ int derive_dense8(Codec &c, size_t n, const uint8_t *present, int goal, std::vec
   cudaFreeAsync(d, s);
   if (cudaStreamSynchronize(s) != cudaSuccess && rc == RSGPU_OK) rc = RSGPU_ERR_CUDA;
   if (rc) return rc;
-  for (size_t i = 0; i < n; ++i) {
-    LeoDenseMap &mp = maps[i];
-    const size_t ni = mp.inputs.size(), nt = mp.targets.size();
-    mp.rows.assign(nt * ni, 0);
-    for (size_t t = 0; t < nt; ++t)
-      for (size_t q = 0; q < ni; ++q) mp.rows[t * ni + q] = host[(i * total + mp.targets[t]) * L + q];
-    auto packed = std::make_shared<std::vector<uint32_t>>(packed_table_words(nt, ni));
-    pack_tables_with(leopard_mul8(), mp.rows.data(), nt, ni, packed->data());
-    mp.packed = std::move(packed);
-  }
+  dense_extract(c, maps, L, host.data());
   return RSGPU_OK;
+}
+
+// Adds derived maps to the codec's map cache (least recently used out
+// beyond kDenseCacheBytes).  Caller holds st.mu.
+void dense_insert_locked(LeopardState &st, const std::string &key, LeoDenseMap &&map) {
+  if (st.dense_index.count(key)) return;
+  const size_t bytes = key.size() + map.rows.size() + map.packed->size() * 4 +
+                       (map.inputs.size() + map.targets.size()) * 2;
+  st.dense_lru.push_front({key, std::make_shared<const LeoDenseMap>(std::move(map)), bytes});
+  st.dense_index.emplace(key, st.dense_lru.begin());
+  st.dense_bytes += bytes;
+  while (st.dense_bytes > kDenseCacheBytes && st.dense_lru.size() > 1) {
+    auto &old = st.dense_lru.back();
+    st.dense_bytes -= old.bytes;
+    st.dense_index.erase(old.key);
+    st.dense_lru.pop_back();
+  }
+}
+
+std::string dense_key(const Codec &c, const uint8_t *present, int goal) {
+  return std::string(reinterpret_cast<const char *>(present), c.k + c.m) + char(goal);
 }
 
 }  // namespace
@@ -1497,8 +1539,7 @@ int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, s
   {
     std::lock_guard<std::mutex> g(st.mu);
     for (size_t i = 0; i < n; ++i) {
-      const std::string key = std::string(reinterpret_cast<const char *>(present + i * total), total) + char(goal);
-      auto it = st.dense_index.find(key);
+      auto it = st.dense_index.find(dense_key(c, present + i * total, goal));
       if (it == st.dense_index.end()) {
         miss.push_back(i);
         continue;
@@ -1516,20 +1557,64 @@ int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, s
   std::lock_guard<std::mutex> g(st.mu);
   for (size_t x = 0; x < miss.size(); ++x) {
     maps[miss[x]] = got[x];
-    std::string key = std::string(reinterpret_cast<const char *>(&pres[x * total]), total) + char(goal);
-    if (st.dense_index.count(key)) continue;
-    const size_t bytes = key.size() + got[x].rows.size() + got[x].packed->size() * 4 +
-                         (got[x].inputs.size() + got[x].targets.size()) * 2;
-    st.dense_lru.push_front({key, std::make_shared<const LeoDenseMap>(std::move(got[x])), bytes});
-    st.dense_index.emplace(std::move(key), st.dense_lru.begin());
-    st.dense_bytes += bytes;
-    while (st.dense_bytes > kDenseCacheBytes && st.dense_lru.size() > 1) {
-      auto &old = st.dense_lru.back();
-      st.dense_bytes -= old.bytes;
-      st.dense_index.erase(old.key);
-      st.dense_lru.pop_back();
-    }
+    dense_insert_locked(st, dense_key(c, &pres[x * total], goal), std::move(got[x]));
   }
+  return RSGPU_OK;
+}
+
+bool leopard_dense_cached(Codec &c, const uint8_t *present, int goal) {
+  LeopardState &st = *c.leo;
+  std::lock_guard<std::mutex> g(st.mu);
+  return st.dense_index.count(dense_key(c, present, goal)) != 0;
+}
+
+size_t leopard_dense_derive_bytes(Codec &c, const uint8_t *present, int goal) {
+  std::vector<LeoDenseMap> maps;
+  return dense_layout(c, 1, present, goal, maps) * (c.k + c.m);
+}
+
+int leopard_dense_derive_start(Codec &c, const uint8_t *present, int goal, uint8_t *pinned, cudaStream_t s,
+                               DenseDerivation &d) {
+  if (c.leo->field->bits != 8) return RSGPU_ERR_INVALID_ARGUMENT;
+  const size_t total = c.k + c.m;
+  std::vector<LeoDenseMap> maps;
+  d.codec = &c;
+  d.goal = goal;
+  d.pattern.assign(reinterpret_cast<const char *>(present), total);
+  d.L = dense_layout(c, 1, present, goal, maps);
+  d.bytes = total * d.L;
+  d.pinned = pinned;
+  dense_units(c, maps, d.L, pinned);
+  RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&d.dev), d.bytes, s)));
+  RS_CUDA(cudaMemcpyAsync(d.dev, pinned, d.bytes, cudaMemcpyHostToDevice, s));
+  std::vector<uint8_t *> ptrs(total);
+  for (size_t i = 0; i < total; ++i) ptrs[i] = d.dev + i * d.L;
+  int rc = run_once(c, RSGPU_OP_RECONSTRUCT, 1, ptrs.data(), present, d.L, goal, nullptr, 0, nullptr, s);
+  if (rc) {
+    cudaFreeAsync(d.dev, s);
+    d.dev = nullptr;
+    return rc;
+  }
+  RS_CUDA(cudaMemcpyAsync(pinned, d.dev, d.bytes, cudaMemcpyDeviceToHost, s));
+  RS_CUDA(cudaFreeAsync(d.dev, s));
+  d.dev = nullptr;
+  RS_CUDA(cudaEventCreateWithFlags(&d.done, cudaEventDisableTiming));
+  return cuda_status(cudaEventRecord(d.done, s));
+}
+
+int leopard_dense_derive_finish(DenseDerivation &d) {
+  const cudaError_t e = cudaEventQuery(d.done);
+  if (e == cudaErrorNotReady) return RSGPU_ERR_INVALID_ARGUMENT;
+  cudaEventDestroy(d.done);
+  d.done = nullptr;
+  if (e != cudaSuccess) return cuda_status(e);
+  Codec &c = *d.codec;
+  std::vector<LeoDenseMap> maps;
+  dense_layout(c, 1, reinterpret_cast<const uint8_t *>(d.pattern.data()), d.goal, maps);
+  dense_extract(c, maps, d.L, d.pinned);
+  LeopardState &st = *c.leo;
+  std::lock_guard<std::mutex> g(st.mu);
+  dense_insert_locked(st, d.pattern + char(d.goal), std::move(maps[0]));
   return RSGPU_OK;
 }
 

@@ -7,6 +7,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "rsgpu.h"
@@ -85,6 +86,27 @@ int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, s
 // maps of more than 16 targets on shards under 1 MiB stay on the FFT decode).
 // Counts this call's bytes towards the pattern's tally.
 bool leopard_dense_due(Codec &c, const uint8_t *present, int goal, size_t len);
+// Whether the codec's map cache holds this pattern's map.
+bool leopard_dense_cached(Codec &c, const uint8_t *present, int goal);
+
+// A map derived off the request path: start queues the FFT decode of the
+// pattern's unit vectors on stream s through a caller-owned pinned buffer of
+// leopard_dense_derive_bytes bytes (no host wait) and records d.done; once
+// d.done has completed, finish packs the map and adds it to the codec's map
+// cache.  The codec must outlive the derivation.
+struct DenseDerivation {
+  Codec *codec = nullptr;
+  std::string pattern;  // k + m presence flags
+  int goal = 0;
+  size_t L = 0, bytes = 0;
+  uint8_t *pinned = nullptr;
+  uint8_t *dev = nullptr;
+  cudaEvent_t done = nullptr;
+};
+size_t leopard_dense_derive_bytes(Codec &c, const uint8_t *present, int goal);
+int leopard_dense_derive_start(Codec &c, const uint8_t *present, int goal, uint8_t *pinned, cudaStream_t s,
+                               DenseDerivation &d);
+int leopard_dense_derive_finish(DenseDerivation &d);
 
 int tower_encode(Codec &c, size_t n_stripes, uint8_t *const *shards, size_t len, cudaStream_t s);
 // Tower-field incremental parity: parity_r (+)= sum_j t[k + r][cols[j]] * inputs[j] (one stripe).

@@ -210,6 +210,7 @@ struct ModelState {
   // seen before launches nothing (its wait would queue behind whatever else
   // occupies the device).  Cleared when the weights change.
   std::unordered_map<std::string, std::vector<float>> memo;
+  uint64_t version = 0;  // counts weight changes
 };
 ModelState &state() {
   static ModelState s;
@@ -261,17 +262,28 @@ int model_set(const float *in, size_t n) {
   state().ready = true;
   state().w_dirty = true;
   state().memo.clear();
+  ++state().version;
   return RSGPU_OK;
 }
 
-int model_predict(const float *features, size_t n, float *out) {
+uint64_t model_version() {
+  std::lock_guard<std::mutex> g(state().mu);
+  return state().version;
+}
+
+int model_predict(const float *features, size_t n, float *out, bool memoize, uint64_t *version) {
   ModelState &m = state();
   std::lock_guard<std::mutex> g(m.mu);
   if (!m.ready) return RSGPU_ERR_INVALID_ARGUMENT;
+  if (version) *version = m.version;
   if (n == 0) return RSGPU_OK;
   // Rows seen before come from the memo; the rest go to the device.
   std::vector<size_t> miss;
   for (size_t i = 0; i < n; ++i) {
+    if (!memoize) {
+      miss.push_back(i);
+      continue;
+    }
     auto it = m.memo.find(std::string(reinterpret_cast<const char *>(features + i * F), F * 4));
     if (it == m.memo.end())
       miss.push_back(i);
@@ -316,11 +328,12 @@ int model_predict(const float *features, size_t n, float *out) {
   RS_CUDA(cudaGetLastError());
   RS_CUDA(cudaMemcpyAsync(m.h_y, m.d_y, n * P * 4, cudaMemcpyDeviceToHost, m.stream));
   RS_CUDA(cudaStreamSynchronize(m.stream));
-  if (m.memo.size() + n > 65536) m.memo.clear();
+  if (memoize && m.memo.size() + n > 65536) m.memo.clear();
   for (size_t x = 0; x < n; ++x) {
     std::memcpy(all_out + miss[x] * P, m.h_y + x * P, P * 4);
-    m.memo.emplace(std::string(reinterpret_cast<const char *>(all + miss[x] * F), F * 4),
-                   std::vector<float>(m.h_y + x * P, m.h_y + (x + 1) * P));
+    if (memoize)
+      m.memo.emplace(std::string(reinterpret_cast<const char *>(all + miss[x] * F), F * 4),
+                     std::vector<float>(m.h_y + x * P, m.h_y + (x + 1) * P));
   }
   return RSGPU_OK;
 }

@@ -5,7 +5,8 @@
 // own request handlers (src/core/encode.rs:935-972,
 // src/core/reconstruct.rs:731-790, src/core/verify.rs:14-174).  This server is
 // the GPU-side loop such a node feeds: requests are submitted from any thread
-// and complete asynchronously.  One worker thread runs the loop:
+// and complete asynchronously.  One worker thread runs the loop (and between
+// its passes, the dense-map derivations of step 4):
 //
 //   1. retire: every launch whose completion event has fired finishes its
 //      requests (verify flags read from pinned memory), frees their device
@@ -17,6 +18,12 @@
 //      stream-ordered device staging, build ONE mixed batch for all admitted
 //      requests (plans from the planner: measured table / cost model), run it
 //      in the persistent kernel, copy outputs back, record an event.
+//
+//   4. derive: a Leopard GF(2^8) rebuild pattern whose dense map has become
+//      due runs the FFT decode in its batch, and its map is derived on a side
+//      stream (queued, never waited for: a wait there queues behind the
+//      persistent batches of the launch streams); a finished derivation adds
+//      the map to its codec's cache, where later batches find it.
 //
 // Up to `streams` launches are in flight at once, so requests that arrive
 // while others run are admitted into the next launch and their work overlaps
@@ -39,9 +46,13 @@
 #include <thread>
 #include <vector>
 
+#include <set>
+#include <string>
+
 #include "batch.hpp"
 #include "codec.hpp"
 #include "handles.hpp"
+#include "leopard.hpp"
 #include "rsgpu.h"
 
 namespace rsgpu {
@@ -158,6 +169,14 @@ class Server {
     }
     cv_.notify_all();
     if (worker_.joinable()) worker_.join();
+    if (dstream_) {
+      cudaStreamSynchronize(dstream_);
+      poll_derivations();
+      cudaStreamDestroy(dstream_);
+      dstream_ = nullptr;
+    }
+    for (auto &p : pinned_pool_) cudaFreeHost(p.first);
+    pinned_pool_.clear();
     for (auto &f : flights_) {
       if (f.stream) cudaStreamSynchronize(f.stream);
       return_slot(device_, f.scratch);  // its stream has finished
@@ -246,6 +265,80 @@ class Server {
   double max_prepare_s_ = 0;  // longest single build-and-launch
   double max_gap_s_ = 0;      // longest time between two passes of the worker loop
   Clock::time_point t0_;
+  // Dense-map derivations in flight on their own stream (step 4), and the
+  // pinned buffers they use (kept until the server stops: freeing pinned
+  // memory synchronizes the device).
+  struct Deriving {
+    DenseDerivation d;
+    std::pair<uint8_t *, size_t> pinned;
+    std::string key;
+  };
+  static constexpr size_t kMaxDerivations = 8;
+  cudaStream_t dstream_ = nullptr;
+  std::vector<Deriving> deriving_;
+  std::vector<DenseWant> wants_;  // filled by mix_build, drained after each launch
+  std::set<std::string> deriving_keys_;
+  std::vector<std::pair<uint8_t *, size_t>> pinned_pool_;
+  uint64_t derived_ = 0;
+
+  // Step 4: queue the derivation of maps that batches found due.
+  void start_derivations(const std::vector<DenseWant> &wants) {
+    for (const DenseWant &w : wants) {
+      if (deriving_.size() >= kMaxDerivations) break;
+      std::string key(reinterpret_cast<const char *>(&w.codec), sizeof(w.codec));
+      key += w.pattern;
+      key += char(w.goal);
+      if (deriving_keys_.count(key)) continue;
+      Codec &c = const_cast<rsgpu_codec *>(w.codec)->c;
+      const uint8_t *pres = reinterpret_cast<const uint8_t *>(w.pattern.data());
+      const size_t need = leopard_dense_derive_bytes(c, pres, w.goal);
+      if (!dstream_ && cudaStreamCreateWithFlags(&dstream_, cudaStreamNonBlocking) != cudaSuccess) return;
+      std::pair<uint8_t *, size_t> buf{nullptr, 0};
+      for (size_t i = 0; i < pinned_pool_.size(); ++i)
+        if (pinned_pool_[i].second >= need) {
+          buf = pinned_pool_[i];
+          pinned_pool_.erase(pinned_pool_.begin() + long(i));
+          break;
+        }
+      if (!buf.first) {
+        if (cudaMallocHost(reinterpret_cast<void **>(&buf.first), need) != cudaSuccess) return;
+        buf.second = need;
+      }
+      Deriving dv;
+      dv.pinned = buf;
+      dv.key = key;
+      if (leopard_dense_derive_start(c, pres, w.goal, buf.first, dstream_, dv.d) != RSGPU_OK) {
+        // The batch already runs this pattern through the FFT decode; only
+        // the map is missing.  Settle the side stream before its buffer is
+        // reused.
+        cudaStreamSynchronize(dstream_);
+        if (dv.d.done) cudaEventDestroy(dv.d.done);
+        pinned_pool_.push_back(buf);
+        continue;
+      }
+      deriving_keys_.insert(key);
+      deriving_.push_back(std::move(dv));
+    }
+  }
+
+  // Finishes the derivations whose work is done.  Returns true on progress.
+  bool poll_derivations() {
+    bool any = false;
+    for (size_t i = 0; i < deriving_.size();) {
+      Deriving &dv = deriving_[i];
+      if (cudaEventQuery(dv.d.done) == cudaErrorNotReady) {
+        ++i;
+        continue;
+      }
+      leopard_dense_derive_finish(dv.d);
+      ++derived_;
+      pinned_pool_.push_back(dv.pinned);
+      deriving_keys_.erase(dv.key);
+      deriving_.erase(deriving_.begin() + long(i));
+      any = true;
+    }
+    return any;
+  }
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0_).count(); }
 
@@ -378,9 +471,13 @@ class Server {
       rsgpu_mix_options_default(&mo);
       mo.planner = opt_.planner;
       mo.graph = 0;
-      rc = mix_build(ops.data(), ops.size(), nullptr, mo, b, f.stream, &f.scratch);
+      rc = mix_build(ops.data(), ops.size(), nullptr, mo, b, f.stream, &f.scratch, &wants_);
     }
     if (rc == RSGPU_OK) rc = mix_launch(*b, f.stream);
+    if (!wants_.empty()) {
+      start_derivations(wants_);
+      wants_.clear();
+    }
     if (rc == RSGPU_OK) {
       for (Req *q : take) {
         if (q->r.mem != RSGPU_MEM_HOST) continue;
@@ -432,6 +529,7 @@ class Server {
       bool progress = retire();
       for (auto &f : flights_)
         if (!f.busy) progress |= admit_and_launch(f);
+      if (!deriving_.empty()) progress |= poll_derivations();
       bool idle_exit = false;
       {
         std::unique_lock<std::mutex> g(mu_);

@@ -152,6 +152,100 @@ bool table_lookup(const rsgpu_mix_op &o, rsgpu_plan *out) {
   return true;
 }
 
+namespace {
+
+// The model's pick over a grid of quantized features, per (family, k, m,
+// operation, goal): shard length in quarter octaves from 64 B, erased / m in
+// 64ths, erased data / erased in 16ths.  A grid is one batched forward pass
+// on the GPU, made the first time an operation of its kind needs the model
+// (and again after the weights change); planning a batch then reads it on the
+// host, so a request path never waits for an inference launch, which would
+// queue behind the persistent batches other streams keep on the device.
+constexpr int kGridLen = 97, kGridErased = 65, kGridData = 17;
+
+struct GridKey {
+  int family, k, m, op, goal;
+  bool operator<(const GridKey &o) const {
+    return std::tie(family, k, m, op, goal) < std::tie(o.family, o.k, o.m, o.op, o.goal);
+  }
+};
+struct Grid {
+  uint64_t version = 0;
+  std::vector<int8_t> best;  // plan index per cell, -1 where no plan is valid
+};
+std::mutex grid_mu;
+std::map<GridKey, Grid> &grids() {
+  static std::map<GridKey, Grid> g;
+  return g;
+}
+
+int grid_cells(int op) { return op == RSGPU_OP_RECONSTRUCT ? kGridLen * kGridErased * kGridData : kGridLen; }
+
+// Cell of an operation, and the features the grid evaluates at that cell.
+int grid_cell(const rsgpu_mix_op &o) {
+  const Codec &c = o.codec->c;
+  const double lg = std::log2(double(std::max<size_t>(o.shard_len, 1)));
+  const int lq = int(std::min<long>(kGridLen - 1, std::max<long>(0, std::lround((lg - 6.0) * 4.0))));
+  if (o.op != RSGPU_OP_RECONSTRUCT) return lq;
+  size_t d = 0;
+  const size_t e = erased(o, &d);
+  const int eq = int(std::lround(64.0 * double(e) / double(c.m)));
+  const int dq = int(std::lround(16.0 * double(d) / double(std::max<size_t>(e, 1))));
+  return (lq * kGridErased + std::min(eq, kGridErased - 1)) * kGridData + std::min(dq, kGridData - 1);
+}
+
+void cell_features(const Codec &c, int op, int cell, float *f) {
+  int lq = cell, eq = 0, dq = 0;
+  if (op == RSGPU_OP_RECONSTRUCT) {
+    dq = cell % kGridData;
+    eq = (cell / kGridData) % kGridErased;
+    lq = cell / (kGridData * kGridErased);
+  }
+  for (int i = 0; i < F; ++i) f[i] = 0.f;
+  f[0] = c.family == RSGPU_FAMILY_CLASSIC ? 1.f : 0.f;
+  f[1] = c.family == RSGPU_FAMILY_LEOPARD_GF8 ? 1.f : 0.f;
+  f[2] = c.family == RSGPU_FAMILY_LEOPARD_GF16 ? 1.f : 0.f;
+  f[3] = float(std::log2(double(c.k)) / 16.0);
+  f[4] = float(std::log2(double(c.m)) / 16.0);
+  f[5] = float((6.0 + lq / 4.0 - 12.0) / 10.0);
+  f[6] = op == RSGPU_OP_ENCODE ? 1.f : 0.f;
+  f[7] = op == RSGPU_OP_RECONSTRUCT ? 1.f : 0.f;
+  f[8] = op == RSGPU_OP_VERIFY ? 1.f : 0.f;
+  f[9] = float(eq / 64.0);
+  f[10] = float(dq / 16.0);
+}
+
+// The grid for op's kind, built when missing or made by older weights.
+int grid_for(const rsgpu_mix_op &o, const Grid **out) {
+  Codec &c = const_cast<rsgpu_codec *>(o.codec)->c;
+  const GridKey key{c.family, int(c.k), int(c.m), o.op, o.op == RSGPU_OP_RECONSTRUCT ? o.goal : 0};
+  const uint64_t version = model_version();
+  std::lock_guard<std::mutex> g(grid_mu);
+  Grid &gr = grids()[key];
+  if (gr.best.empty() || gr.version != version) {
+    const int cells = grid_cells(o.op);
+    std::vector<float> feat(size_t(cells) * F), pred(size_t(cells) * P);
+    for (int x = 0; x < cells; ++x) cell_features(c, o.op, x, &feat[size_t(x) * F]);
+    uint64_t v = 0;
+    int rc = model_predict(feat.data(), cells, pred.data(), false, &v);
+    if (rc) return rc;
+    gr.best.assign(cells, -1);
+    for (int x = 0; x < cells; ++x) {
+      int best = -1;
+      for (int j = 0; j < P; ++j) {
+        if (!mix_plan_valid(c, o.op, plan_of_index(j))) continue;
+        if (best < 0 || pred[size_t(x) * P + j] > pred[size_t(x) * P + best]) best = j;
+      }
+      gr.best[x] = int8_t(best);
+    }
+    gr.version = v;
+  }
+  *out = &gr;  // std::map nodes are stable
+  return RSGPU_OK;
+}
+
+}  // namespace
+
 int mix_plan_batch(const rsgpu_mix_op *ops, size_t n, int planner, std::vector<rsgpu_plan> &plans) {
   if (planner == RSGPU_PLANNER_FIXED) return RSGPU_OK;
   std::vector<size_t> ask;
@@ -164,20 +258,12 @@ int mix_plan_batch(const rsgpu_mix_op *ops, size_t n, int planner, std::vector<r
       ask.push_back(i);
   }
   if (ask.empty() || !model_ready()) return RSGPU_OK;
-  std::vector<float> feat(ask.size() * F), pred(ask.size() * P);
-  for (size_t x = 0; x < ask.size(); ++x) plan_features(ops[ask[x]], &feat[x * F]);
-  int rc = model_predict(feat.data(), ask.size(), pred.data());
-  if (rc) return rc;
-  for (size_t x = 0; x < ask.size(); ++x) {
-    const rsgpu_mix_op &o = ops[ask[x]];
-    Codec &c = const_cast<rsgpu_codec *>(o.codec)->c;
-    int best = -1;
-    for (int j = 0; j < P; ++j) {
-      const rsgpu_plan p = plan_of_index(j);
-      if (!mix_plan_valid(c, o.op, p)) continue;
-      if (best < 0 || pred[x * P + j] > pred[x * P + best]) best = j;
-    }
-    if (best >= 0) plans[ask[x]] = plan_of_index(best);
+  for (size_t i : ask) {
+    const Grid *g = nullptr;
+    int rc = grid_for(ops[i], &g);
+    if (rc) return rc;
+    const int best = g->best[grid_cell(ops[i])];
+    if (best >= 0) plans[i] = plan_of_index(best);
   }
   return RSGPU_OK;
 }
