@@ -803,9 +803,10 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   std::memcpy(host.data() + o_leo, B.leo_jobs.data(), B.leo_jobs.size() * sizeof(LeoJob));
   std::memcpy(host.data() + o_roles, B.roles.data(), B.roles.size());
   std::memcpy(host.data() + o_tbl, B.tables.data(), B.tables.size() * 4);
-  if (b.stream_ordered)  // pageable source: staged before the call returns
-    RS_CUDA(cudaMemcpyAsync(b.d_blob, host.data(), host.size(), cudaMemcpyHostToDevice, b.stream));
-  else
+  if (b.stream_ordered) {  // through pinned memory: never waits for the stream's earlier work
+    const int rc = upload_to(b.d_blob, host.data(), host.size(), b.stream);
+    if (rc) return rc;
+  } else
     RS_CUDA(cudaMemcpy(b.d_blob, host.data(), host.size(), cudaMemcpyHostToDevice));
 
   // ---- launch shape

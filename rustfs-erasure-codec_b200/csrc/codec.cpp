@@ -38,10 +38,11 @@ struct UploadSlot {
     if (host) cudaFreeHost(host);
   }
 };
-// A small ring per thread, so an upload waits only for the copy issued
+// A ring per thread, so an upload waits only for the copy issued
 // kUploadSlots uploads earlier (a call that uploads tables and then its job
-// blob does not wait for its own first copy).
-constexpr int kUploadSlots = 8;
+// blob does not wait for its own first copy, and a request server's worker,
+// which builds batches for several streams in turn, rarely waits at all).
+constexpr int kUploadSlots = 32;
 thread_local UploadSlot t_upload[kUploadSlots];
 thread_local int t_upload_next = 0;
 
@@ -79,10 +80,16 @@ int lib_malloc_async(void **p, size_t bytes, void *stream) {
 
 namespace {
 
-// Copies `bytes` of host data to a fresh stream-ordered device allocation
-// through a pinned, event-guarded bounce buffer.  The device block is freed
-// stream-ordered by the caller.
-int upload(const void *src, size_t bytes, void **dev, cudaStream_t s) {
+}  // namespace
+
+// Copies `bytes` of host data to device memory `dst`, stream-ordered on s,
+// through a pinned, event-guarded bounce buffer.  A copy from pageable memory
+// could instead block the calling thread until the stream reached it (the
+// driver stages large pageable copies in a bounded buffer), i.e. behind
+// whatever the stream waits for.
+int upload_to(void *dst, const void *src, size_t bytes, void *stream) {
+  if (!bytes) return RSGPU_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   UploadSlot &u = t_upload[t_upload_next];
   t_upload_next = (t_upload_next + 1) % kUploadSlots;
   if (!u.done) RS_CUDA(cudaEventCreateWithFlags(&u.done, cudaEventDisableTiming));
@@ -98,10 +105,17 @@ int upload(const void *src, size_t bytes, void **dev, cudaStream_t s) {
     u.cap = cap;
   }
   std::memcpy(u.host, src, bytes);
-  RS_CUDA(cudaError_t(lib_malloc_async(dev, std::max<size_t>(bytes, 16), s)));
-  RS_CUDA(cudaMemcpyAsync(*dev, u.host, bytes, cudaMemcpyHostToDevice, s));
+  RS_CUDA(cudaMemcpyAsync(dst, u.host, bytes, cudaMemcpyHostToDevice, s));
   RS_CUDA(cudaEventRecord(u.done, s));
   return RSGPU_OK;
+}
+
+namespace {
+// Copies `bytes` of host data to a fresh stream-ordered device allocation
+// (upload_to).  The device block is freed stream-ordered by the caller.
+int upload(const void *src, size_t bytes, void **dev, cudaStream_t s) {
+  RS_CUDA(cudaError_t(lib_malloc_async(dev, std::max<size_t>(bytes, 16), s)));
+  return upload_to(*dev, src, bytes, s);
 }
 }  // namespace
 

@@ -60,5 +60,9 @@ inline int lib_malloc_async(T **p, size_t bytes, void *stream) {
 }
 // The pool itself (cudaMemPool_t), for cudaMallocFromPoolAsync callers.
 int lib_pool(void **out);
+// Host -> device copy, stream-ordered on `stream`, through a pinned bounce
+// buffer of the calling thread (never blocks on the stream's earlier work).
+// Returns an RSGPU_* code.
+int upload_to(void *dst, const void *src, size_t bytes, void *stream);
 
 }  // namespace rsgpu

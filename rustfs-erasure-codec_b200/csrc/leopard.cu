@@ -749,7 +749,8 @@ int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>
   // Stream-ordered scratch: nothing here waits for other streams' work.
   uint8_t *d_pres = nullptr;
   RS_CUDA(cudaError_t(lib_malloc_async(reinterpret_cast<void **>(&d_pres), pres.size(), s)));
-  RS_CUDA(cudaMemcpyAsync(d_pres, pres.data(), pres.size(), cudaMemcpyHostToDevice, s));
+  int rc = upload_to(d_pres, pres.data(), pres.size(), s);
+  if (rc) return rc;
   std::vector<const uint8_t *> pp(pending.size());
   std::vector<uint16_t *> oo(pending.size());
   for (size_t i = 0; i < pending.size(); ++i) {
@@ -759,8 +760,8 @@ int build_locators(Codec &c, std::vector<std::pair<std::string, const uint8_t *>
   void *d_pp = nullptr, *d_oo = nullptr;
   RS_CUDA(cudaError_t(lib_malloc_async(&d_pp, pp.size() * sizeof(void *), s)));
   RS_CUDA(cudaError_t(lib_malloc_async(&d_oo, oo.size() * sizeof(void *), s)));
-  RS_CUDA(cudaMemcpyAsync(d_pp, pp.data(), pp.size() * sizeof(void *), cudaMemcpyHostToDevice, s));
-  RS_CUDA(cudaMemcpyAsync(d_oo, oo.data(), oo.size() * sizeof(void *), cudaMemcpyHostToDevice, s));
+  if ((rc = upload_to(d_pp, pp.data(), pp.size() * sizeof(void *), s))) return rc;
+  if ((rc = upload_to(d_oo, oo.data(), oo.size() * sizeof(void *), s))) return rc;
   const int bits = st.field->bits;
   const size_t smem = size_t(1u << bits) * 2;
   if (bits == 16) {
@@ -916,10 +917,11 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
       jobs[i].err = locs + size_t(slot_of_job[i]) * st.n;
     }
     std::memcpy(blob.data(), jobs.data(), jb);
-    if (one_shot)
-      RS_CUDA(cudaMemcpyAsync(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, s));
-    else
+    if (one_shot) {
+      if ((rc = upload_to(L.d_blob, blob.data(), blob.size(), s))) return rc;
+    } else {
       RS_CUDA(cudaMemcpy(L.d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+    }
     if ((rc = copy_locators(st, used, locs, s, one_shot))) return rc;
   }
   const size_t jb = jobs.size() * sizeof(LeoJob);
