@@ -38,13 +38,19 @@ struct UploadSlot {
     if (host) cudaFreeHost(host);
   }
 };
-// A ring per thread, so an upload waits only for the copy issued
-// kUploadSlots uploads earlier (a call that uploads tables and then its job
-// blob does not wait for its own first copy, and a request server's worker,
-// which builds batches for several streams in turn, rarely waits at all).
-constexpr int kUploadSlots = 32;
-thread_local UploadSlot t_upload[kUploadSlots];
-thread_local int t_upload_next = 0;
+// Bounce buffers per thread.  A buffer is reused once the copy last issued
+// from it has completed (an event query, never a wait), else another buffer
+// is taken or a new one allocated: the copies are stream-ordered, and a
+// stream may wait a long time behind other streams' persistent kernels.
+// Buffers are not freed while the thread runs (freeing pinned memory
+// synchronizes the device), except when the pool is full and no free buffer
+// is large enough, which a steady workload reaches only while warming up.
+constexpr size_t kUploadSlots = 64;
+struct UploadPool {
+  std::vector<std::unique_ptr<UploadSlot>> slots;
+  size_t next = 0;
+};
+thread_local UploadPool t_upload;
 
 }  // namespace
 
@@ -90,23 +96,44 @@ namespace {
 int upload_to(void *dst, const void *src, size_t bytes, void *stream) {
   if (!bytes) return RSGPU_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  UploadSlot &u = t_upload[t_upload_next];
-  t_upload_next = (t_upload_next + 1) % kUploadSlots;
-  if (!u.done) RS_CUDA(cudaEventCreateWithFlags(&u.done, cudaEventDisableTiming));
-  RS_CUDA(cudaEventSynchronize(u.done));  // previous upload from this thread has left the buffer
-  if (u.cap < bytes) {
-    if (u.host) cudaFreeHost(u.host);
-    u.host = nullptr;
-    // Geometric growth: freeing pinned memory synchronizes the device, so it
-    // should happen a handful of times per thread, not per call.
-    size_t cap = std::max<size_t>(u.cap * 2, 1 << 20);
-    while (cap < bytes) cap <<= 1;
-    RS_CUDA(cudaHostAlloc(&u.host, cap, cudaHostAllocDefault));
-    u.cap = cap;
+  UploadPool &pool = t_upload;
+  UploadSlot *u = nullptr, *small = nullptr;
+  const size_t n = pool.slots.size();
+  for (size_t i = 0; i < n && !u; ++i) {  // first fit, starting after the last slot used
+    UploadSlot *x = pool.slots[(pool.next + i) % n].get();
+    if (cudaEventQuery(x->done) == cudaErrorNotReady) continue;
+    if (x->cap >= bytes) {
+      u = x;
+      pool.next = (pool.next + i + 1) % n;
+    } else if (!small) {
+      small = x;
+    }
   }
-  std::memcpy(u.host, src, bytes);
-  RS_CUDA(cudaMemcpyAsync(dst, u.host, bytes, cudaMemcpyHostToDevice, s));
-  RS_CUDA(cudaEventRecord(u.done, s));
+  cudaGetLastError();  // a not-ready query is not an error
+  if (!u) {
+    size_t cap = size_t(1) << 20;
+    while (cap < bytes) cap <<= 1;
+    if (pool.slots.size() < kUploadSlots) {
+      pool.slots.emplace_back(new UploadSlot());
+      u = pool.slots.back().get();
+      RS_CUDA(cudaEventCreateWithFlags(&u->done, cudaEventDisableTiming));
+    } else {
+      u = small ? small : pool.slots[pool.next].get();
+      RS_CUDA(cudaEventSynchronize(u->done));  // every buffer is in flight: wait for one
+      if (u->cap < bytes) {
+        cudaFreeHost(u->host);
+        u->host = nullptr;
+        u->cap = 0;
+      }
+    }
+    if (!u->host) {
+      RS_CUDA(cudaHostAlloc(&u->host, cap, cudaHostAllocDefault));
+      u->cap = cap;
+    }
+  }
+  std::memcpy(u->host, src, bytes);
+  RS_CUDA(cudaMemcpyAsync(dst, u->host, bytes, cudaMemcpyHostToDevice, s));
+  RS_CUDA(cudaEventRecord(u->done, s));
   return RSGPU_OK;
 }
 
