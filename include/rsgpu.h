@@ -483,6 +483,13 @@ int32_t rsgpu_model_ready(void);
  * Host-memory requests (pinned memory recommended) are staged through device
  * memory: inputs in, outputs (parity, rebuilt shards) back into the caller's
  * buffers; device-memory requests (shards resident in HBM) run in place.
+ * The planner reads the cost model's picks from a grid of predictions over
+ * quantized features (made by one batched GPU forward pass per operation kind
+ * and weight set), and a Leopard GF(2^8) rebuild pattern whose dense map has
+ * become due runs the FFT decode while the server derives the map on a side
+ * stream, so building a batch never waits for the GPU.  Codecs must outlive
+ * the server (a map derivation may still use one after its requests are
+ * done).
  * Shard buffers must stay untouched until the request completes.  Results
  * are byte-identical to the per-call entry points whatever else is in the
  * batch.  No reference counterpart: the reference is called once per stripe
