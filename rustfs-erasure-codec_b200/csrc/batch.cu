@@ -658,6 +658,7 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
       a.skew = g.skew;
       a.bank = g.bank;
       a.kbank = g.kbank;
+      a.sktab = g.sktab;
       a.st_ienc = g.st_ienc;
       a.st_fenc = g.st_fenc;
       a.st_idec = g.st_idec;

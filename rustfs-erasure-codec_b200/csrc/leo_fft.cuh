@@ -96,16 +96,25 @@ struct Kc {
   KTab<BITS> t;
 };
 
+// skew: the field's FFT skew logs; sktab: the multiplier tables of each skew
+// entry (entry i = the bank's tables of log skew[i]).  A transform's skew
+// base is an offset into both.
 struct FftCtx {
   const uint32_t *bank;
   uint32_t mod;
   uint32_t lane;
+  const uint16_t *skew;
+  const uint32_t *sktab;
 };
 
+// The butterfly constant at skew entry skb + idx.  Its log (for the
+// reference's skip of a multiply by a log-modulus constant) and its tables
+// are independent loads, so their latencies overlap; with the tables looked
+// up by log value instead, the table load had to wait for the log.
 template <int BITS>
-__device__ __forceinline__ Kc<BITS> kc(const FftCtx &x, const uint16_t *skb, uint32_t idx) {
-  const uint32_t lm = __ldg(skb + idx);
-  return Kc<BITS>{lm, kload<BITS>(x.bank, lm, x.lane)};
+__device__ __forceinline__ Kc<BITS> kc(const FftCtx &x, int32_t skb, uint32_t idx) {
+  const uint32_t i = uint32_t(skb + int32_t(idx));
+  return Kc<BITS>{__ldg(x.skew + i), kload<BITS>(x.sktab, i, x.lane)};
 }
 
 // Inverse butterfly (IFFT): y ^= x; x ^= y * c.  Forward (FFT): x ^= y * c; y ^= x.
@@ -141,15 +150,15 @@ __device__ __forceinline__ void fq(uint32_t &a, uint32_t &b, uint32_t &c, uint32
 }
 
 // One stage on the registers v[0..G) holding lanes R + a + dm * j.  skb is
-// the transform's skew base: a radix-4 block starting at lane r with distance
-// d uses skb[r + d], skb[r + 2d], skb[r + 3d] (m01, m02, m23); a radix-2
-// block uses skb[r + d].  LG = log2 G; FWD selects FFT (true) or IFFT.
+// the transform's skew base (an offset into the field's skew entries): a
+// radix-4 block starting at lane r with distance d uses entries skb + r + d,
+// skb + r + 2d, skb + r + 3d (m01, m02, m23); a radix-2 block uses skb + r + d.  LG = log2 G; FWD selects FFT (true) or IFFT.
 //   IFFT: G=16: radix-4 (d = dm) then radix-4 (4dm); G=8: radix-4 (dm) then
 //         radix-2 (4dm); G=4: radix-4 (dm); G=2: radix-2 (dm).
 //   FFT:  G=16: radix-4 (4dm) then radix-4 (dm); G=8: radix-4 (2dm) then
 //         radix-2 (dm); G=4: radix-4 (dm); G=2: radix-2 (dm).
 template <int BITS, int LG, bool FWD>
-__device__ __forceinline__ void stage_regs(uint32_t *v, const FftCtx &x, const uint16_t *skb, uint32_t R,
+__device__ __forceinline__ void stage_regs(uint32_t *v, const FftCtx &x, int32_t skb, uint32_t R,
                                            uint32_t dm) {
   const uint32_t mod = x.mod;
   if (LG == 4) {
@@ -218,7 +227,7 @@ __device__ __forceinline__ void stage_regs(uint32_t *v, const FftCtx &x, const u
 }
 
 template <int BITS, bool FWD>
-__device__ __forceinline__ void stage_regs_rt(uint32_t *v, int lg, const FftCtx &x, const uint16_t *skb, uint32_t R,
+__device__ __forceinline__ void stage_regs_rt(uint32_t *v, int lg, const FftCtx &x, int32_t skb, uint32_t R,
                                               uint32_t dm) {
   switch (lg) {
     case 4: stage_regs<BITS, 4, FWD>(v, x, skb, R, dm); break;
@@ -274,7 +283,7 @@ __device__ __forceinline__ uint8_t st_at(uint32_t plan, uint32_t s) { return uin
 // shape is a template parameter so that each loop body is straight-line code.
 template <int BITS, bool FWD, int LG, int NT>
 __device__ __forceinline__ void smem_stage_lg(uint32_t *S, uint32_t C, uint32_t lgC32, uint32_t L, uint32_t lgdm,
-                                              const FftCtx &x, const uint16_t *skb, uint32_t mtrunc) {
+                                              const FftCtx &x, int32_t skb, uint32_t mtrunc) {
   constexpr uint32_t G = 1u << LG;
   const uint32_t dm = 1u << lgdm;
   const uint32_t warp = threadIdx.x >> 5;
@@ -296,7 +305,7 @@ __device__ __forceinline__ void smem_stage_lg(uint32_t *S, uint32_t C, uint32_t 
 
 template <int BITS, bool FWD, int NT>
 __device__ __forceinline__ void smem_stage(uint32_t *S, uint32_t C, uint32_t lgC32, uint32_t L, uint8_t st,
-                                        const FftCtx &x, const uint16_t *skb, uint32_t mtrunc) {
+                                        const FftCtx &x, int32_t skb, uint32_t mtrunc) {
   const uint32_t lgdm = st >> 3;
   switch (st_lg(st)) {
     case 4: smem_stage_lg<BITS, FWD, 4, NT>(S, C, lgC32, L, lgdm, x, skb, mtrunc); break;
@@ -350,7 +359,7 @@ namespace {
 template <int BITS, int NT>
 __device__ __forceinline__ void enc_stage0(uint32_t *dst, bool accumulate, const LeoArgs &a, const uint8_t *const *ptr,
                                         uint32_t g, uint32_t cnt, uint32_t C, uint32_t lgC32, uint64_t col0,
-                                        uint64_t len, const FftCtx &x, const uint16_t *skb) {
+                                        uint64_t len, const FftCtx &x, int32_t skb) {
   const uint32_t warp = threadIdx.x >> 5, m = a.m;
   const uint32_t items = (m >> 4) << lgC32;
   for (uint32_t it = warp; it < items; it += NT / 32) {
@@ -378,7 +387,7 @@ __device__ __forceinline__ void enc_stage0(uint32_t *dst, bool accumulate, const
 template <int BITS, int LG, int NT>
 __device__ __forceinline__ void enc_last_ifft_lg(const uint32_t *T, uint32_t *A, bool accumulate, uint32_t C,
                                                  uint32_t lgC32, uint32_t m, uint32_t lgdm, const FftCtx &x,
-                                                 const uint16_t *skb) {
+                                                 int32_t skb) {
   constexpr uint32_t G = 1u << LG;
   const uint32_t dm = 1u << lgdm, warp = threadIdx.x >> 5;
   const uint32_t items = (m >> LG) << lgC32;
@@ -402,7 +411,7 @@ __device__ __forceinline__ void enc_last_ifft_lg(const uint32_t *T, uint32_t *A,
 template <int BITS, int NT>
 __device__ __forceinline__ void enc_last_ifft(const uint32_t *T, uint32_t *A, bool accumulate, uint32_t C,
                                            uint32_t lgC32, uint32_t m, uint8_t st, const FftCtx &x,
-                                           const uint16_t *skb) {
+                                           int32_t skb) {
   const uint32_t lgdm = st >> 3;
   switch (st_lg(st)) {
     case 4: enc_last_ifft_lg<BITS, 4, NT>(T, A, accumulate, C, lgC32, m, lgdm, x, skb); break;
@@ -417,7 +426,7 @@ __device__ __forceinline__ void enc_last_ifft(const uint32_t *T, uint32_t *A, bo
 template <int BITS, bool VERIFY, int LG, int NT>
 __device__ __forceinline__ uint32_t enc_out_lg(const uint32_t *A, const LeoArgs &a, const uint8_t *const *ptr,
                                                uint32_t C, uint32_t lgC32, uint64_t col0, uint64_t len,
-                                               const FftCtx &x, const uint16_t *skf) {
+                                               const FftCtx &x, int32_t skf) {
   constexpr uint32_t G = 1u << LG;
   const uint32_t warp = threadIdx.x >> 5, m = a.m, p = a.p, k = a.k;
   const uint32_t items = (m >> LG) << lgC32;
@@ -450,7 +459,7 @@ __device__ __forceinline__ uint32_t enc_out_lg(const uint32_t *A, const LeoArgs 
 template <int BITS, bool VERIFY, int NT>
 __device__ __forceinline__ uint32_t enc_out(const uint32_t *A, const LeoArgs &a, const uint8_t *const *ptr, uint32_t C,
                                          uint32_t lgC32, uint8_t st, uint64_t col0, uint64_t len, const FftCtx &x,
-                                         const uint16_t *skf) {
+                                         int32_t skf) {
   switch (st_lg(st)) {
     case 4: return enc_out_lg<BITS, VERIFY, 4, NT>(A, a, ptr, C, lgC32, col0, len, x, skf);
     case 3: return enc_out_lg<BITS, VERIFY, 3, NT>(A, a, ptr, C, lgC32, col0, len, x, skf);
@@ -480,11 +489,11 @@ __device__ __forceinline__ uint32_t enc_regs_lg(const LeoArgs &a, const uint8_t 
       if (j < cnt && act) w = ldg_u32(ptr[g * M + j] + col);
       v[j] = fft_to_work<BITS>(w, x.lane);
     }
-    stage_regs<BITS, LG, false>(v, x, a.skew + (M - 1) + g * M, 0, 1);
+    stage_regs<BITS, LG, false>(v, x, int32_t(M - 1 + g * M), 0, 1);
 #pragma unroll
     for (uint32_t j = 0; j < M; ++j) acc[j] ^= v[j];
   }
-  stage_regs<BITS, LG, true>(acc, x, a.skew - 1, 0, 1);
+  stage_regs<BITS, LG, true>(acc, x, -1, 0, 1);
   uint32_t mismatch = 0;
 #pragma unroll
   for (uint32_t j = 0; j < M; ++j) {
@@ -527,7 +536,7 @@ template <int BITS, bool VERIFY, int NT>
 __device__ void fft_encode_tile(uint32_t *W, const LeoArgs &a, const LeoJob &jd, uint64_t col0, uint64_t len,
                                 uint32_t *bad) {
   const uint32_t lane = threadIdx.x & 31;
-  const FftCtx x{a.kbank, a.mod, lane};
+  const FftCtx x{a.kbank, a.mod, lane, a.skew, a.sktab};
   const uint32_t m = a.m, k = a.k;
   const uint8_t *const *ptr = a.ptrs + jd.ptr_off;
   uint32_t mismatch = 0;
@@ -542,7 +551,7 @@ __device__ void fft_encode_tile(uint32_t *W, const LeoArgs &a, const LeoJob &jd,
     uint32_t *T = W, *A = W + size_t(m) * C;
     for (uint32_t g = 0; g * m < k; ++g) {
       const uint32_t cnt = min(m, k - g * m);
-      const uint16_t *skb = a.skew + (m - 1) + g * m;
+      const int32_t skb = int32_t(m - 1 + g * m);
       enc_stage0<BITS, NT>(T, false, a, ptr, g, cnt, C, lgC32, col0, len, x, skb);
       __syncthreads();
       for (uint32_t s = 1; s + 1 < a.n_ienc; ++s) {
@@ -553,7 +562,7 @@ __device__ void fft_encode_tile(uint32_t *W, const LeoArgs &a, const LeoJob &jd,
       __syncthreads();
     }
     // FFT over the accumulator; the last stage (consecutive lanes) writes parity.
-    const uint16_t *skf = a.skew - 1;
+    const int32_t skf = -1;
     for (uint32_t s = 0; s + 1 < a.n_fenc; ++s) {
       smem_stage<BITS, true, NT>(A, C, lgC32, m, st_at(a.st_fenc, s), x, skf, a.p);
       __syncthreads();
@@ -605,7 +614,7 @@ __device__ __forceinline__ void dec_store(const LeoArgs &a, const LeoJob &jd, co
 template <int BITS, int NT>
 __device__ __forceinline__ void dec_stage0(uint32_t *S, const LeoArgs &a, const LeoJob &jd, const uint8_t *const *ptr,
                                         uint32_t C, uint32_t lgC32, uint64_t col0, uint64_t len, const FftCtx &x,
-                                        const uint16_t *skd) {
+                                        int32_t skd) {
   const uint32_t warp = threadIdx.x >> 5, in_cnt = jd.input_count;
   const uint32_t items = (a.n >> 4) << lgC32;
   for (uint32_t it = warp; it < items; it += NT / 32) {
@@ -630,7 +639,7 @@ __device__ __forceinline__ void dec_stage0(uint32_t *S, const LeoArgs &a, const 
 template <int BITS, int LG, int NT>
 __device__ __forceinline__ void dec_out_lg(const uint32_t *S, const LeoArgs &a, const LeoJob &jd,
                                            const uint8_t *const *ptr, uint32_t C, uint32_t lgC32, uint64_t col0,
-                                           uint64_t len, const FftCtx &x, const uint16_t *skd) {
+                                           uint64_t len, const FftCtx &x, int32_t skd) {
   constexpr uint32_t G = 1u << LG;
   const uint32_t warp = threadIdx.x >> 5, out_cnt = a.m + a.k;
   const uint32_t items = (a.n >> LG) << lgC32;
@@ -651,7 +660,7 @@ __device__ __forceinline__ void dec_out_lg(const uint32_t *S, const LeoArgs &a, 
 template <int BITS, int NT>
 __device__ __forceinline__ void dec_out(const uint32_t *S, const LeoArgs &a, const LeoJob &jd, const uint8_t *const *ptr,
                                      uint32_t C, uint32_t lgC32, uint8_t st, uint64_t col0, uint64_t len,
-                                     const FftCtx &x, const uint16_t *skd) {
+                                     const FftCtx &x, int32_t skd) {
   switch (st_lg(st)) {
     case 4: dec_out_lg<BITS, 4, NT>(S, a, jd, ptr, C, lgC32, col0, len, x, skd); break;
     case 3: dec_out_lg<BITS, 3, NT>(S, a, jd, ptr, C, lgC32, col0, len, x, skd); break;
@@ -667,7 +676,7 @@ __device__ __forceinline__ void dec_regs_lg(const LeoArgs &a, const LeoJob &jd, 
   constexpr uint32_t N = 1u << LG;
   const uint64_t col = col0 + 4ull * threadIdx.x;
   const bool act = col < len;
-  const uint16_t *skd = a.skew - 1;
+  const int32_t skd = -1;
   uint32_t v[16];
 #pragma unroll
   for (uint32_t j = 0; j < 16; ++j) v[j] = j < N ? dec_load<BITS>(a, jd, ptr, j, col, act, x) : 0u;
@@ -698,10 +707,10 @@ __device__ __forceinline__ void dec_regs(const LeoArgs &a, const LeoJob &jd, con
 template <int BITS, int NT>
 __device__ void fft_decode_tile(uint32_t *W, const LeoArgs &a, const LeoJob &jd, uint64_t col0, uint64_t len) {
   const uint32_t lane = threadIdx.x & 31;
-  const FftCtx x{a.kbank, a.mod, lane};
+  const FftCtx x{a.kbank, a.mod, lane, a.skew, a.sktab};
   const uint32_t n = a.n;
   const uint8_t *const *ptr = a.ptrs + jd.ptr_off;
-  const uint16_t *skd = a.skew - 1;
+  const int32_t skd = -1;
   if (n <= 16) {
     dec_regs<BITS>(a, jd, ptr, col0, len, x);
     __syncthreads();

@@ -39,6 +39,7 @@ struct LeoArgs {
   // lanes-per-thread | log2 dm << 3); packed words, not byte arrays, so that
   // device code indexes them with shifts instead of a local-memory copy.
   const uint32_t *kbank;
+  const uint32_t *sktab;  // kbank's tables of each skew entry (entry i: log skew[i])
   uint32_t st_ienc, st_fenc, st_idec, st_fdec;
   uint32_t n_ienc, n_fenc, n_idec, n_fdec;
 };

@@ -148,6 +148,7 @@ struct LeoField {
   uint16_t *d_walsh = nullptr;
   uint32_t *d_bank = nullptr;   // multiplier tables indexed by log value (half-warp layer kernels)
   uint32_t *d_kbank = nullptr;  // tables of the register-stage kernels (GF(2^8): 5+3 split; GF(2^16): d_bank)
+  uint32_t *d_sktab = nullptr;  // d_kbank's entry of each skew entry: entry i holds the tables of log skew[i]
   explicit LeoField(int b) : bits(b), host(b) {}
 };
 
@@ -191,8 +192,18 @@ static int leo_field(int bits, LeoField **out) {
       }
       RS_CUDA(cudaMalloc(&f->d_kbank, kb.size() * 4));
       RS_CUDA(cudaMemcpy(f->d_kbank, kb.data(), kb.size() * 4, cudaMemcpyHostToDevice));
+      std::vector<uint32_t> sk(size_t(t.mod) * kWBank8);
+      for (uint32_t i = 0; i < t.mod; ++i)
+        std::memcpy(&sk[size_t(i) * kWBank8], &kb[size_t(t.skew[i]) * kWBank8], kWBank8 * 4);
+      RS_CUDA(cudaMalloc(&f->d_sktab, sk.size() * 4));
+      RS_CUDA(cudaMemcpy(f->d_sktab, sk.data(), sk.size() * 4, cudaMemcpyHostToDevice));
     } else {
       f->d_kbank = f->d_bank;
+      const size_t w = 16 * words;  // one entry: 16 lanes x 4 words
+      std::vector<uint32_t> sk(size_t(t.mod) * w);
+      for (uint32_t i = 0; i < t.mod; ++i) std::memcpy(&sk[size_t(i) * w], &bank[size_t(t.skew[i]) * w], w * 4);
+      RS_CUDA(cudaMalloc(&f->d_sktab, sk.size() * 4));
+      RS_CUDA(cudaMemcpy(f->d_sktab, sk.data(), sk.size() * 4, cudaMemcpyHostToDevice));
     }
     fields[slot] = f;
   }
@@ -942,6 +953,7 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
   a.last = st.last;
   a.mod = st.field->host.mod;
   a.kbank = st.field->d_kbank;
+  a.sktab = st.field->d_sktab;
   fill_stages(a);
   L.engine = leo_engine();
   if (L.engine == 1) {
@@ -1312,6 +1324,7 @@ int leopard_geometry(Codec &c, LeoGeometry *g) {
   g->skew = st.field->d_skew;
   g->bank = st.field->d_bank;
   g->kbank = st.field->d_kbank;
+  g->sktab = st.field->d_sktab;
   LeoArgs a{};
   a.m = st.m;
   a.n = st.n;

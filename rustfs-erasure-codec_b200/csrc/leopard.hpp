@@ -48,6 +48,7 @@ struct LeoGeometry {
   const uint16_t *skew;
   const uint32_t *bank;   // half-warp layer kernels
   const uint32_t *kbank;  // register-stage kernels
+  const uint32_t *sktab;  // kbank's tables of each skew entry
   uint32_t st_ienc, st_fenc, st_idec, st_fdec;  // stage plans (leo_types.hpp)
   uint32_t n_ienc, n_fenc, n_idec, n_fdec;
 };
