@@ -691,6 +691,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_apply_tma (10+4 encode, 4096 x 1 MiB)",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "frac_of_nominal_8tbs": round(achieved / 8000.0, 4),
                          "traffic": None if ratio is None else int(enc_bytes * ratio),
                          "algorithmic_bytes": enc_bytes},
             "per_stripe": {"value": round(ps_value, 1), "unit": "GB/s", "stripes_per_geometry": n_ps,
@@ -794,6 +795,10 @@ def leopard16_workload(torch, rsgpu, stream, gen):
     mism = int((buf != orig).sum())
     cols = size // 2
     mx = {"encode": (2 * 256 * 9 + 256 * 9) * cols * n, "reconstruct": 2 * 1024 * 11 * cols * n}
+    # Shuffle bound of a GF(2^16) multiply-XOR: 8 table shuffles per 32-bit
+    # word (two elements), one warp-wide shuffle per SM clock.
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    bound = props.multi_processor_count * 1.965e9 * 32 / 8 * 2
     nbytes = n * (k + m) * size  # encode reads k, writes m; reconstruct reads k + m - e, writes e
     out = {"workload": "Leopard GF16 1024+512, 16 KiB shards, 64 stripes, 512 seeded erasures each",
            "bit_exact": mism == 0, "mismatched_bytes": mism}
@@ -802,7 +807,9 @@ def leopard16_workload(torch, rsgpu, stream, gen):
         out[name] = {"ms": round(med, 3), "p99_ms": round(p99, 3),
                      "gbs": round(nbytes / (med / 1e3) / 1e9, 1),
                      "data_gibs": round(n * k * size / (med / 1e3) / 2**30, 1),
-                     "mul_xor_per_s": float(f"{mx[name] / (med / 1e3):.4g}")}
+                     "mul_xor_per_s": float(f"{mx[name] / (med / 1e3):.4g}"),
+                     "frac_of_shuffle_bound": round(mx[name] / (med / 1e3) / bound, 3)}
+    out["shuffle_bound_mul_xor_per_s"] = float(f"{bound:.4g}")
     out["mismatched_bytes"] += int((buf != orig).sum())
     out["bit_exact"] = out["mismatched_bytes"] == 0
     del buf, orig

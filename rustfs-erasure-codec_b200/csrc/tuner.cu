@@ -215,7 +215,10 @@ void cell_features(const Codec &c, int op, int cell, float *f) {
   f[10] = float(dq / 16.0);
 }
 
-// The grid for op's kind, built when missing or made by older weights.
+// The grid for op's kind, built when missing or made by older weights.  The
+// grids of every kind of the codec's shape (encode, verify, reconstruct with
+// goal all and data) are built together, in one forward pass, so a serving
+// stream meets at most one build per codec shape.
 int grid_for(const rsgpu_mix_op &o, const Grid **out) {
   Codec &c = const_cast<rsgpu_codec *>(o.codec)->c;
   const GridKey key{c.family, int(c.k), int(c.m), o.op, o.op == RSGPU_OP_RECONSTRUCT ? o.goal : 0};
@@ -223,22 +226,39 @@ int grid_for(const rsgpu_mix_op &o, const Grid **out) {
   std::lock_guard<std::mutex> g(grid_mu);
   Grid &gr = grids()[key];
   if (gr.best.empty() || gr.version != version) {
-    const int cells = grid_cells(o.op);
-    std::vector<float> feat(size_t(cells) * F), pred(size_t(cells) * P);
-    for (int x = 0; x < cells; ++x) cell_features(c, o.op, x, &feat[size_t(x) * F]);
+    struct Kind {
+      int op, goal;
+    };
+    const Kind kinds[4] = {{RSGPU_OP_ENCODE, 0},
+                           {RSGPU_OP_VERIFY, 0},
+                           {RSGPU_OP_RECONSTRUCT, RSGPU_GOAL_ALL},
+                           {RSGPU_OP_RECONSTRUCT, RSGPU_GOAL_DATA}};
+    std::vector<float> feat;
+    size_t rows = 0;
+    for (const Kind &kd : kinds) rows += size_t(grid_cells(kd.op));
+    feat.resize(rows * F);
+    std::vector<float> pred(rows * P);
+    size_t at = 0;
+    for (const Kind &kd : kinds)
+      for (int x = 0; x < grid_cells(kd.op); ++x, ++at) cell_features(c, kd.op, x, &feat[at * F]);
     uint64_t v = 0;
-    int rc = model_predict(feat.data(), cells, pred.data(), false, &v);
+    int rc = model_predict(feat.data(), rows, pred.data(), false, &v);
     if (rc) return rc;
-    gr.best.assign(cells, -1);
-    for (int x = 0; x < cells; ++x) {
-      int best = -1;
-      for (int j = 0; j < P; ++j) {
-        if (!mix_plan_valid(c, o.op, plan_of_index(j))) continue;
-        if (best < 0 || pred[size_t(x) * P + j] > pred[size_t(x) * P + best]) best = j;
+    at = 0;
+    for (const Kind &kd : kinds) {
+      Grid &kg = grids()[GridKey{c.family, int(c.k), int(c.m), kd.op, kd.goal}];
+      const int cells = grid_cells(kd.op);
+      kg.best.assign(cells, -1);
+      for (int x = 0; x < cells; ++x, ++at) {
+        int best = -1;
+        for (int j = 0; j < P; ++j) {
+          if (!mix_plan_valid(c, kd.op, plan_of_index(j))) continue;
+          if (best < 0 || pred[at * P + j] > pred[at * P + best]) best = j;
+        }
+        kg.best[x] = int8_t(best);
       }
-      gr.best[x] = int8_t(best);
+      kg.version = v;
     }
-    gr.version = v;
   }
   *out = &gr;  // std::map nodes are stable
   return RSGPU_OK;
