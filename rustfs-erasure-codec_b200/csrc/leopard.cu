@@ -233,6 +233,25 @@ __global__ void __launch_bounds__(kLeoThreads) k_leo_encode(LeoArgs a) {
 }
 
 constexpr int kFftThreads = 256;
+// Tiles whose shared memory allows one CTA per SM run one "wide" CTA of
+// kWideThreads threads per SM; transforms whose work rows live in global
+// memory run kGlobalBlocks CTAs of kWideThreads per SM.  Registers per thread:
+// 65536 / (threads per SM).  The transforms are latency-bound (long-scoreboard
+// waits on the constant tables and work rows dominate their stalls), so warps
+// count for more than registers: at 1024 threads (64 registers, a few hundred
+// bytes of spills) the config-3 GF(2^16) 1024+512 encode runs in 3.26 ms and
+// the decode in 12.16 ms, against 4.48 and 16.83 ms at 512 threads (128
+// registers); 2048+1024 at 8 KiB: 3.96 / 14.16 against 5.17 / 19.85 ms.  Two
+// 512-thread CTAs per SM for global work rows gave 12.76 ms (decode), and
+// 1024-thread CTAs two per SM (32 registers) spill kilobytes.
+constexpr int kWideThreads = 1024;
+// Other tiles run kNarrowBlocks CTAs of kFftThreads per SM, each within
+// kFftSmemBudget bytes of shared memory: four (64 registers, narrower column
+// tiles) rather than two (128 registers) made every such transform faster,
+// e.g. GF(2^16) 300+100 at 64 KiB 4.19 / 15.66 -> 3.17 / 11.62 ms (encode /
+// decode, 64 stripes), GF(2^8) 32+16 at 1 MiB decode 18.46 -> 13.00 ms.
+constexpr int kNarrowBlocks = 4;
+constexpr int kGlobalBlocks = 1;
 
 // Register-stage kernels (leo_fft.cuh).  Tile: 4 * kFftThreads bytes when the
 // transform fits in registers (m or n <= 16), else 64 * nb bytes with the
@@ -241,10 +260,10 @@ __host__ __device__ inline uint64_t fft_tile_bytes(uint32_t lanes_one_thread, ui
   return lanes_one_thread <= 16 ? uint64_t(4 * kFftThreads) : uint64_t(64) * nb;
 }
 
-// NT = 512 is used when a tile's shared memory leaves room for one CTA per
-// SM: 16 warps instead of 8 on the same rows, at the same 128-register cap.
+// NT = kWideThreads is used when a tile's shared memory leaves room for one
+// CTA per SM, and for work rows in global memory.
 template <int BITS, bool VERIFY, bool GLOBAL_WORK, int NT = kFftThreads>
-__global__ void __launch_bounds__(NT, NT == kFftThreads ? 2 : 1) k_fft_encode(LeoArgs a) {
+__global__ void __launch_bounds__(NT, NT == kFftThreads ? kNarrowBlocks : (GLOBAL_WORK ? kGlobalBlocks : 1)) k_fft_encode(LeoArgs a) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint32_t bad;
   uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
@@ -260,7 +279,7 @@ __global__ void __launch_bounds__(NT, NT == kFftThreads ? 2 : 1) k_fft_encode(Le
 }
 
 template <int BITS, bool GLOBAL_WORK, int NT = kFftThreads>
-__global__ void __launch_bounds__(NT, NT == kFftThreads ? 2 : 1) k_fft_decode(LeoArgs a) {
+__global__ void __launch_bounds__(NT, NT == kFftThreads ? kNarrowBlocks : (GLOBAL_WORK ? kGlobalBlocks : 1)) k_fft_decode(LeoArgs a) {
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t *W = GLOBAL_WORK ? a.scratch + size_t(blockIdx.x) * a.lanes * a.nb * kRowWords : smem;
   const uint64_t tile_bytes = fft_tile_bytes(a.n, a.nb);
@@ -439,7 +458,7 @@ struct LeoLaunch {
   // after the kernel; prepared launches own it until destroyed.
   bool blob_ordered = false;
   cudaStream_t blob_stream = nullptr;
-  int threads = 256;  // register-stage kernels: 256, or 512 for one CTA per SM
+  int threads = 256;  // register-stage kernels: 256, or kWideThreads for one CTA per SM
   int grid = 0;
   size_t smem = 0;
   bool global_work = false;
@@ -590,7 +609,7 @@ int &leo_engine() {
 
 namespace {
 
-constexpr size_t kFftSmemBudget = 96 * 1024;  // two resident CTAs per SM
+constexpr size_t kFftSmemBudget = (192 * 1024) / kNarrowBlocks;  // kNarrowBlocks resident CTAs per SM
 
 // Work rows and tile width of a register-stage launch: `rows` rows of work
 // (encoder 2m, decoder n) when the transform needs shared memory, i.e. when
@@ -614,8 +633,8 @@ int configure_fft(const K kernel, const K2 kernel_wide, LeoLaunch &L, uint32_t r
   if (!L.global_work) {
     L.smem = smem;
     const void *fn = reinterpret_cast<const void *>(kernel);
-    if (smem > kFftSmemBudget) {  // one CTA per SM: give it twice the warps
-      L.threads = 2 * kFftThreads;
+    if (smem > kFftSmemBudget) {  // one CTA per SM: give it more warps
+      L.threads = kWideThreads;
       fn = reinterpret_cast<const void *>(kernel_wide);
     }
     RS_CUDA(ensure_smem_limit(fn, smem));
@@ -623,11 +642,11 @@ int configure_fft(const K kernel, const K2 kernel_wide, LeoLaunch &L, uint32_t r
     RS_CUDA(blocks_per_sm(fn, L.threads, smem, &per_sm));
     L.grid = int(std::min<uint64_t>(tiles, uint64_t(std::max(per_sm, 1)) * sm_count()));
   } else {
-    // Work rows in a global slab (L2-resident): one 512-thread CTA per SM
-    // keeps the slab half the size of two 256-thread CTAs per SM.
+    // Work rows in a global slab (L2-resident): one wide CTA per SM keeps the
+    // slab smaller than several narrower CTAs would.
     L.smem = 0;
-    L.threads = 2 * kFftThreads;
-    L.grid = int(std::min<uint64_t>(tiles, uint64_t(sm_count())));
+    L.threads = kWideThreads;
+    L.grid = int(std::min<uint64_t>(tiles, uint64_t(kGlobalBlocks) * sm_count()));
     const size_t need = size_t(L.grid) * rows * nb * 64;
     int rc = grow_scratch(st, need);
     if (rc) return rc;
@@ -960,16 +979,16 @@ int build_leo(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const 
     const bool b16f = st.field->bits == 16;
     const size_t nj = jobs.size();
     if (L.decode)
-      return b16f ? configure_fft(k_fft_decode<16, false>, k_fft_decode<16, false, 512>, L, st.n, st.n, len, nj)
-                  : configure_fft(k_fft_decode<8, false>, k_fft_decode<8, false, 512>, L, st.n, st.n, len, nj);
+      return b16f ? configure_fft(k_fft_decode<16, false>, k_fft_decode<16, false, kWideThreads>, L, st.n, st.n, len, nj)
+                  : configure_fft(k_fft_decode<8, false>, k_fft_decode<8, false, kWideThreads>, L, st.n, st.n, len, nj);
     if (L.verify)
-      return b16f ? configure_fft(k_fft_encode<16, true, false>, k_fft_encode<16, true, false, 512>, L, 2 * st.m,
+      return b16f ? configure_fft(k_fft_encode<16, true, false>, k_fft_encode<16, true, false, kWideThreads>, L, 2 * st.m,
                                   st.m, len, nj)
-                  : configure_fft(k_fft_encode<8, true, false>, k_fft_encode<8, true, false, 512>, L, 2 * st.m, st.m,
+                  : configure_fft(k_fft_encode<8, true, false>, k_fft_encode<8, true, false, kWideThreads>, L, 2 * st.m, st.m,
                                   len, nj);
-    return b16f ? configure_fft(k_fft_encode<16, false, false>, k_fft_encode<16, false, false, 512>, L, 2 * st.m,
+    return b16f ? configure_fft(k_fft_encode<16, false, false>, k_fft_encode<16, false, false, kWideThreads>, L, 2 * st.m,
                                 st.m, len, nj)
-                : configure_fft(k_fft_encode<8, false, false>, k_fft_encode<8, false, false, 512>, L, 2 * st.m, st.m,
+                : configure_fft(k_fft_encode<8, false, false>, k_fft_encode<8, false, false, kWideThreads>, L, 2 * st.m, st.m,
                                 len, nj);
   }
   const uint32_t lanes = L.decode ? st.n : 2 * st.m;
@@ -1025,25 +1044,25 @@ int leo_launch_kernel(const LeoLaunch &L, cudaStream_t s) {
 #define FFT_GO(KERNEL) KERNEL<<<grid, block, L.smem, s>>>(a)
     if (L.decode) {
       if (L.global_work) {
-        if (b16) FFT_GO((k_fft_decode<16, true, 512>)); else FFT_GO((k_fft_decode<8, true, 512>));
+        if (b16) FFT_GO((k_fft_decode<16, true, kWideThreads>)); else FFT_GO((k_fft_decode<8, true, kWideThreads>));
       } else if (wide) {
-        if (b16) FFT_GO((k_fft_decode<16, false, 512>)); else FFT_GO((k_fft_decode<8, false, 512>));
+        if (b16) FFT_GO((k_fft_decode<16, false, kWideThreads>)); else FFT_GO((k_fft_decode<8, false, kWideThreads>));
       } else {
         if (b16) FFT_GO((k_fft_decode<16, false>)); else FFT_GO((k_fft_decode<8, false>));
       }
     } else if (L.verify) {
       if (L.global_work) {
-        if (b16) FFT_GO((k_fft_encode<16, true, true, 512>)); else FFT_GO((k_fft_encode<8, true, true, 512>));
+        if (b16) FFT_GO((k_fft_encode<16, true, true, kWideThreads>)); else FFT_GO((k_fft_encode<8, true, true, kWideThreads>));
       } else if (wide) {
-        if (b16) FFT_GO((k_fft_encode<16, true, false, 512>)); else FFT_GO((k_fft_encode<8, true, false, 512>));
+        if (b16) FFT_GO((k_fft_encode<16, true, false, kWideThreads>)); else FFT_GO((k_fft_encode<8, true, false, kWideThreads>));
       } else {
         if (b16) FFT_GO((k_fft_encode<16, true, false>)); else FFT_GO((k_fft_encode<8, true, false>));
       }
     } else {
       if (L.global_work) {
-        if (b16) FFT_GO((k_fft_encode<16, false, true, 512>)); else FFT_GO((k_fft_encode<8, false, true, 512>));
+        if (b16) FFT_GO((k_fft_encode<16, false, true, kWideThreads>)); else FFT_GO((k_fft_encode<8, false, true, kWideThreads>));
       } else if (wide) {
-        if (b16) FFT_GO((k_fft_encode<16, false, false, 512>)); else FFT_GO((k_fft_encode<8, false, false, 512>));
+        if (b16) FFT_GO((k_fft_encode<16, false, false, kWideThreads>)); else FFT_GO((k_fft_encode<8, false, false, kWideThreads>));
       } else {
         if (b16) FFT_GO((k_fft_encode<16, false, false>)); else FFT_GO((k_fft_encode<8, false, false>));
       }
