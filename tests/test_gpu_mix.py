@@ -187,12 +187,13 @@ def test_mix_every_plan_writes_the_same_bytes(rs, torch, codecs, variant):
     assert list(mb.results()) == flags
 
 
-@pytest.mark.parametrize("size,want_tile", [(4096, 1), (196608, 3)])
+@pytest.mark.parametrize("size,want_tile", [(4096, 1), (262144, 3)])
 def test_small_batch_runs_transforms_at_the_finest_tile(rs, torch, codecs, size, want_tile):
     # The fixed rule gives a 128+64 encode 8 blocks per work item.  A batch
-    # with fewer items than the kernel's resident CTAs (one 4 KiB stripe: 8
-    # items) runs at the finest tile instead, so more items run side by side;
-    # one that fills the GPU (192 KiB: 384 items) keeps the planned tile.
+    # with fewer items than the kernel's resident CTAs (3 x 148; one 4 KiB
+    # stripe: 8 items) runs at the finest tile instead, so more items run side
+    # by side; one that fills the GPU (256 KiB: 512 items) keeps the planned
+    # tile.
     # The bytes are the oracle's either way.
     g = ("leopard_gf8", 128, 64)
     c = codecs[g]
