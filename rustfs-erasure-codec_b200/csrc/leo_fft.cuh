@@ -22,8 +22,11 @@
 //     c*i held one entry per lane (one shuffle per byte); the high three bits
 //     select, with one byte-permute for all four bytes of a word, from an
 //     8-entry byte table of c*(h << 5) held in two registers.
-//   GF(2^16): four 16-entry nibble tables per constant (c * (n << 4q)), one
-//     shuffle per nibble, both elements of a word at once (the split byte
+//   GF(2^16): 5+5+5+1 split.  Bits 0-4, 5-9 and 10-14 of each element index
+//     three 32-entry tables (c * (i << 5q)) held one entry per lane (one
+//     shuffle each, so six per word of two elements, against eight for
+//     nibble tables); bit 15 of both elements becomes a mask with one
+//     sign-replicating byte-permute, applied to c * 2^15 (the split byte
 //     layout is converted to 16-bit elements on load and back on store).
 //
 // Which lanes a stage may skip: the reference only runs the butterflies of
@@ -53,7 +56,7 @@ struct KTab<8> {
 };
 template <>
 struct KTab<16> {
-  uint32_t t0, t1, t2, t3;
+  uint32_t t0, t1, t2, c15;  // c * (lane << 0 / 5 / 10) and c * 2^15, each in both halves
 };
 
 // GF(2^8) table bank, one record of kWBank8 words per log value:
@@ -69,9 +72,10 @@ __device__ __forceinline__ KTab<8> kload<8>(const uint32_t *bank, uint32_t lm, u
   const uint2 h = __ldg(reinterpret_cast<const uint2 *>(r + 32));
   return KTab<8>{__ldg(r + lane), h.x, h.y};
 }
+// GF(2^16) table bank, one record of 32 lanes x 4 words per log value.
 template <>
 __device__ __forceinline__ KTab<16> kload<16>(const uint32_t *bank, uint32_t lm, uint32_t lane) {
-  const uint4 v = __ldg(reinterpret_cast<const uint4 *>(bank) + lm * 16 + (lane & 15));
+  const uint4 v = __ldg(reinterpret_cast<const uint4 *>(bank) + lm * 32 + lane);
   return KTab<16>{v.x, v.y, v.z, v.w};
 }
 
@@ -83,10 +87,18 @@ __device__ __forceinline__ uint32_t kmul(uint32_t w, const KTab<8> &t) {
   const uint32_t lo = __byte_perm(__byte_perm(s0, s1, 0x0040), __byte_perm(s2, s3, 0x4000), 0x7610);
   return lo ^ __byte_perm(t.h0, t.h1, hi3_selector(w));
 }
+// Byte permute with sign replication: selector nibble 9 (B) fills a byte
+// with the top bit of source byte 1 (3).  __byte_perm reads only three
+// bits of each selector nibble, so this is written in PTX.
+__device__ __forceinline__ uint32_t top_bit_masks(uint32_t w) {
+  uint32_t r;
+  asm("prmt.b32 %0, %1, 0, 0xBB99;" : "=r"(r) : "r"(w));
+  return r;  // low half: bit 15 of w replicated, high half: bit 31
+}
 __device__ __forceinline__ uint32_t kmul(uint32_t w, const KTab<16> &t) {
-  const uint32_t a = tshfl(t.t0, w) ^ tshfl(t.t1, w >> 4) ^ tshfl(t.t2, w >> 8) ^ tshfl(t.t3, w >> 12);
-  const uint32_t b = tshfl(t.t0, w >> 16) ^ tshfl(t.t1, w >> 20) ^ tshfl(t.t2, w >> 24) ^ tshfl(t.t3, w >> 28);
-  return __byte_perm(a, b, 0x7610);
+  const uint32_t a = tshfl(t.t0, w) ^ tshfl(t.t1, w >> 5) ^ tshfl(t.t2, w >> 10);
+  const uint32_t b = tshfl(t.t0, w >> 16) ^ tshfl(t.t1, w >> 21) ^ tshfl(t.t2, w >> 26);
+  return __byte_perm(a, b, 0x7610) ^ (top_bit_masks(w) & t.c15);
 }
 
 // Warp-uniform butterfly constant: its log value and this thread's tables.
@@ -111,42 +123,44 @@ struct FftCtx {
 // reference's skip of a multiply by a log-modulus constant) and its tables
 // are independent loads, so their latencies overlap; with the tables looked
 // up by log value instead, the table load had to wait for the log.
-template <int BITS>
+// SK = false: the caller knows that no constant of its group has that log,
+// so the log is not loaded and every butterfly multiplies.
+template <int BITS, bool SK>
 __device__ __forceinline__ Kc<BITS> kc(const FftCtx &x, int32_t skb, uint32_t idx) {
   const uint32_t i = uint32_t(skb + int32_t(idx));
-  return Kc<BITS>{__ldg(x.skew + i), kload<BITS>(x.sktab, i, x.lane)};
+  return Kc<BITS>{SK ? uint32_t(__ldg(x.skew + i)) : 0u, kload<BITS>(x.sktab, i, x.lane)};
 }
 
 // Inverse butterfly (IFFT): y ^= x; x ^= y * c.  Forward (FFT): x ^= y * c; y ^= x.
-template <int BITS>
+template <int BITS, bool SK>
 __device__ __forceinline__ void ibf(uint32_t &x, uint32_t &y, const Kc<BITS> &c, uint32_t mod) {
   y ^= x;
-  if (c.lm != mod) x ^= kmul(y, c.t);
+  if (!SK || c.lm != mod) x ^= kmul(y, c.t);
 }
-template <int BITS>
+template <int BITS, bool SK>
 __device__ __forceinline__ void fbf(uint32_t &x, uint32_t &y, const Kc<BITS> &c, uint32_t mod) {
-  if (c.lm != mod) x ^= kmul(y, c.t);
+  if (!SK || c.lm != mod) x ^= kmul(y, c.t);
   y ^= x;
 }
 
 // Radix-4 on (a, b, c, d) = lanes i, i+d, i+2d, i+3d of one block.
 // Inverse order: (a,b) m01, (c,d) m23, (a,c) m02, (b,d) m02.
 // Forward order: (a,c) m02, (b,d) m02, (a,b) m01, (c,d) m23.
-template <int BITS>
+template <int BITS, bool SK>
 __device__ __forceinline__ void iq(uint32_t &a, uint32_t &b, uint32_t &c, uint32_t &d, const Kc<BITS> &m01,
                                    const Kc<BITS> &m02, const Kc<BITS> &m23, uint32_t mod) {
-  ibf<BITS>(a, b, m01, mod);
-  ibf<BITS>(c, d, m23, mod);
-  ibf<BITS>(a, c, m02, mod);
-  ibf<BITS>(b, d, m02, mod);
+  ibf<BITS, SK>(a, b, m01, mod);
+  ibf<BITS, SK>(c, d, m23, mod);
+  ibf<BITS, SK>(a, c, m02, mod);
+  ibf<BITS, SK>(b, d, m02, mod);
 }
-template <int BITS>
+template <int BITS, bool SK>
 __device__ __forceinline__ void fq(uint32_t &a, uint32_t &b, uint32_t &c, uint32_t &d, const Kc<BITS> &m01,
                                    const Kc<BITS> &m02, const Kc<BITS> &m23, uint32_t mod) {
-  fbf<BITS>(a, c, m02, mod);
-  fbf<BITS>(b, d, m02, mod);
-  fbf<BITS>(a, b, m01, mod);
-  fbf<BITS>(c, d, m23, mod);
+  fbf<BITS, SK>(a, c, m02, mod);
+  fbf<BITS, SK>(b, d, m02, mod);
+  fbf<BITS, SK>(a, b, m01, mod);
+  fbf<BITS, SK>(c, d, m23, mod);
 }
 
 // One stage on the registers v[0..G) holding lanes R + a + dm * j.  skb is
@@ -157,34 +171,34 @@ __device__ __forceinline__ void fq(uint32_t &a, uint32_t &b, uint32_t &c, uint32
 //         radix-2 (4dm); G=4: radix-4 (dm); G=2: radix-2 (dm).
 //   FFT:  G=16: radix-4 (4dm) then radix-4 (dm); G=8: radix-4 (2dm) then
 //         radix-2 (dm); G=4: radix-4 (dm); G=2: radix-2 (dm).
-template <int BITS, int LG, bool FWD>
-__device__ __forceinline__ void stage_regs(uint32_t *v, const FftCtx &x, int32_t skb, uint32_t R,
-                                           uint32_t dm) {
+template <int BITS, int LG, bool FWD, bool SK>
+__device__ __forceinline__ void stage_regs_k(uint32_t *v, const FftCtx &x, int32_t skb, uint32_t R,
+                                             uint32_t dm) {
   const uint32_t mod = x.mod;
   if (LG == 4) {
     if (!FWD) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
         const uint32_t r = R + 4 * s * dm;
-        const Kc<BITS> m01 = kc<BITS>(x, skb, r + dm), m02 = kc<BITS>(x, skb, r + 2 * dm),
-                       m23 = kc<BITS>(x, skb, r + 3 * dm);
-        iq<BITS>(v[4 * s], v[4 * s + 1], v[4 * s + 2], v[4 * s + 3], m01, m02, m23, mod);
+        const Kc<BITS> m01 = kc<BITS, SK>(x, skb, r + dm), m02 = kc<BITS, SK>(x, skb, r + 2 * dm),
+                       m23 = kc<BITS, SK>(x, skb, r + 3 * dm);
+        iq<BITS, SK>(v[4 * s], v[4 * s + 1], v[4 * s + 2], v[4 * s + 3], m01, m02, m23, mod);
       }
-      const Kc<BITS> m01 = kc<BITS>(x, skb, R + 4 * dm), m02 = kc<BITS>(x, skb, R + 8 * dm),
-                     m23 = kc<BITS>(x, skb, R + 12 * dm);
+      const Kc<BITS> m01 = kc<BITS, SK>(x, skb, R + 4 * dm), m02 = kc<BITS, SK>(x, skb, R + 8 * dm),
+                     m23 = kc<BITS, SK>(x, skb, R + 12 * dm);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) iq<BITS>(v[t], v[t + 4], v[t + 8], v[t + 12], m01, m02, m23, mod);
+      for (int t = 0; t < 4; ++t) iq<BITS, SK>(v[t], v[t + 4], v[t + 8], v[t + 12], m01, m02, m23, mod);
     } else {
-      const Kc<BITS> m01 = kc<BITS>(x, skb, R + 4 * dm), m02 = kc<BITS>(x, skb, R + 8 * dm),
-                     m23 = kc<BITS>(x, skb, R + 12 * dm);
+      const Kc<BITS> m01 = kc<BITS, SK>(x, skb, R + 4 * dm), m02 = kc<BITS, SK>(x, skb, R + 8 * dm),
+                     m23 = kc<BITS, SK>(x, skb, R + 12 * dm);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) fq<BITS>(v[t], v[t + 4], v[t + 8], v[t + 12], m01, m02, m23, mod);
+      for (int t = 0; t < 4; ++t) fq<BITS, SK>(v[t], v[t + 4], v[t + 8], v[t + 12], m01, m02, m23, mod);
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
         const uint32_t r = R + 4 * s * dm;
-        const Kc<BITS> n01 = kc<BITS>(x, skb, r + dm), n02 = kc<BITS>(x, skb, r + 2 * dm),
-                       n23 = kc<BITS>(x, skb, r + 3 * dm);
-        fq<BITS>(v[4 * s], v[4 * s + 1], v[4 * s + 2], v[4 * s + 3], n01, n02, n23, mod);
+        const Kc<BITS> n01 = kc<BITS, SK>(x, skb, r + dm), n02 = kc<BITS, SK>(x, skb, r + 2 * dm),
+                       n23 = kc<BITS, SK>(x, skb, r + 3 * dm);
+        fq<BITS, SK>(v[4 * s], v[4 * s + 1], v[4 * s + 2], v[4 * s + 3], n01, n02, n23, mod);
       }
     }
   } else if (LG == 3) {
@@ -192,38 +206,66 @@ __device__ __forceinline__ void stage_regs(uint32_t *v, const FftCtx &x, int32_t
 #pragma unroll
       for (int s = 0; s < 2; ++s) {
         const uint32_t r = R + 4 * s * dm;
-        const Kc<BITS> m01 = kc<BITS>(x, skb, r + dm), m02 = kc<BITS>(x, skb, r + 2 * dm),
-                       m23 = kc<BITS>(x, skb, r + 3 * dm);
-        iq<BITS>(v[4 * s], v[4 * s + 1], v[4 * s + 2], v[4 * s + 3], m01, m02, m23, mod);
+        const Kc<BITS> m01 = kc<BITS, SK>(x, skb, r + dm), m02 = kc<BITS, SK>(x, skb, r + 2 * dm),
+                       m23 = kc<BITS, SK>(x, skb, r + 3 * dm);
+        iq<BITS, SK>(v[4 * s], v[4 * s + 1], v[4 * s + 2], v[4 * s + 3], m01, m02, m23, mod);
       }
-      const Kc<BITS> c = kc<BITS>(x, skb, R + 4 * dm);
+      const Kc<BITS> c = kc<BITS, SK>(x, skb, R + 4 * dm);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) ibf<BITS>(v[t], v[t + 4], c, mod);
+      for (int t = 0; t < 4; ++t) ibf<BITS, SK>(v[t], v[t + 4], c, mod);
     } else {
-      const Kc<BITS> m01 = kc<BITS>(x, skb, R + 2 * dm), m02 = kc<BITS>(x, skb, R + 4 * dm),
-                     m23 = kc<BITS>(x, skb, R + 6 * dm);
+      const Kc<BITS> m01 = kc<BITS, SK>(x, skb, R + 2 * dm), m02 = kc<BITS, SK>(x, skb, R + 4 * dm),
+                     m23 = kc<BITS, SK>(x, skb, R + 6 * dm);
 #pragma unroll
-      for (int t = 0; t < 2; ++t) fq<BITS>(v[t], v[t + 2], v[t + 4], v[t + 6], m01, m02, m23, mod);
+      for (int t = 0; t < 2; ++t) fq<BITS, SK>(v[t], v[t + 2], v[t + 4], v[t + 6], m01, m02, m23, mod);
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
-        const Kc<BITS> c = kc<BITS>(x, skb, R + 2 * s * dm + dm);
-        fbf<BITS>(v[2 * s], v[2 * s + 1], c, mod);
+        const Kc<BITS> c = kc<BITS, SK>(x, skb, R + 2 * s * dm + dm);
+        fbf<BITS, SK>(v[2 * s], v[2 * s + 1], c, mod);
       }
     }
   } else if (LG == 2) {
-    const Kc<BITS> m01 = kc<BITS>(x, skb, R + dm), m02 = kc<BITS>(x, skb, R + 2 * dm),
-                   m23 = kc<BITS>(x, skb, R + 3 * dm);
+    const Kc<BITS> m01 = kc<BITS, SK>(x, skb, R + dm), m02 = kc<BITS, SK>(x, skb, R + 2 * dm),
+                   m23 = kc<BITS, SK>(x, skb, R + 3 * dm);
     if (!FWD)
-      iq<BITS>(v[0], v[1], v[2], v[3], m01, m02, m23, mod);
+      iq<BITS, SK>(v[0], v[1], v[2], v[3], m01, m02, m23, mod);
     else
-      fq<BITS>(v[0], v[1], v[2], v[3], m01, m02, m23, mod);
+      fq<BITS, SK>(v[0], v[1], v[2], v[3], m01, m02, m23, mod);
   } else if (LG == 1) {
-    const Kc<BITS> c = kc<BITS>(x, skb, R + dm);
+    const Kc<BITS> c = kc<BITS, SK>(x, skb, R + dm);
     if (!FWD)
-      ibf<BITS>(v[0], v[1], c, mod);
+      ibf<BITS, SK>(v[0], v[1], c, mod);
     else
-      fbf<BITS>(v[0], v[1], c, mod);
+      fbf<BITS, SK>(v[0], v[1], c, mod);
   }
+}
+
+// True when a constant of the group of lanes R + a + dm * j (j < G) may be a
+// skew entry whose log is the field modulus.  Those entries are exactly
+// 2^i - 1 in both fields' skew tables (checked when the tables are built),
+// and the group's constants are entries skb + R + dm * t, 0 < t < G, so the
+// question is whether base + dm * t, base = skb + 1 + R, is a power of two
+// for such a t.  A power of two of at least dm is a multiple of dm, so base
+// must be one, and then base / dm + t must be a power of two.
+__device__ __forceinline__ bool group_may_skip(int32_t skb, uint32_t R, uint32_t dm, uint32_t G) {
+  const uint32_t base = uint32_t(skb + 1) + R;
+  if (base & (dm - 1)) return false;
+  const uint32_t q = base / dm + 1;  // smallest candidate
+  const uint32_t p2 = q <= 1 ? 1u : 1u << (32 - __clz(q - 1));
+  return p2 <= q + G - 2;
+}
+
+// One register stage (see stage_regs_k).  GF(2^16): groups that cannot meet
+// a skipped multiply run without the per-butterfly test (the choice is
+// warp-uniform).  GF(2^8) keeps the test everywhere: the second copy of every
+// stage body made its decodes 5-8% slower (config-4 shapes, B200), the
+// encodes 3-6% faster.
+template <int BITS, int LG, bool FWD>
+__device__ __forceinline__ void stage_regs(uint32_t *v, const FftCtx &x, int32_t skb, uint32_t R, uint32_t dm) {
+  if (BITS == 8 || group_may_skip(skb, R, dm, 1u << LG))
+    stage_regs_k<BITS, LG, FWD, true>(v, x, skb, R, dm);
+  else
+    stage_regs_k<BITS, LG, FWD, false>(v, x, skb, R, dm);
 }
 
 template <int BITS, bool FWD>

@@ -147,7 +147,7 @@ struct LeoField {
   uint16_t *d_skew = nullptr;
   uint16_t *d_walsh = nullptr;
   uint32_t *d_bank = nullptr;   // multiplier tables indexed by log value (half-warp layer kernels)
-  uint32_t *d_kbank = nullptr;  // tables of the register-stage kernels (GF(2^8): 5+3 split; GF(2^16): d_bank)
+  uint32_t *d_kbank = nullptr;  // tables of the register-stage kernels (GF(2^8): 5+3 split; GF(2^16): 5+5+5+1)
   uint32_t *d_sktab = nullptr;  // d_kbank's entry of each skew entry: entry i holds the tables of log skew[i]
   explicit LeoField(int b) : bits(b), host(b) {}
 };
@@ -160,6 +160,14 @@ static int leo_field(int bits, LeoField **out) {
   if (!fields[slot]) {
     LeoField *f = new LeoField(bits);
     const LeoTables &t = f->host;
+    // The transforms test for a skipped multiply (a skew entry whose log is
+    // the modulus) only in groups that can meet one, on the property that
+    // those entries are exactly 2^i - 1.
+    for (uint32_t i = 0; i < t.mod; ++i)
+      if ((t.skew[i] == t.mod) != (((i + 1) & i) == 0)) {
+        delete f;
+        return RSGPU_ERR_CUDA;
+      }
     RS_CUDA(cudaMalloc(&f->d_skew, t.skew.size() * 2));
     RS_CUDA(cudaMemcpy(f->d_skew, t.skew.data(), t.skew.size() * 2, cudaMemcpyHostToDevice));
     RS_CUDA(cudaMalloc(&f->d_walsh, t.walsh.size() * 2));
@@ -198,10 +206,21 @@ static int leo_field(int bits, LeoField **out) {
       RS_CUDA(cudaMalloc(&f->d_sktab, sk.size() * 4));
       RS_CUDA(cudaMemcpy(f->d_sktab, sk.data(), sk.size() * 4, cudaMemcpyHostToDevice));
     } else {
-      f->d_kbank = f->d_bank;
-      const size_t w = 16 * words;  // one entry: 16 lanes x 4 words
+      // Per log value, 32 lanes x 4 words (layout of leo_fft.cuh): c * i,
+      // c * (i << 5), c * (i << 10) for i = lane, and c * 2^15, each
+      // replicated into both 16-bit halves.
+      const size_t w = 32 * 4;
+      std::vector<uint32_t> kb(size_t(t.order) * w);
+      for (uint32_t lm = 0; lm < t.order; ++lm)
+        for (uint32_t i = 0; i < 32; ++i) {
+          uint32_t *e = &kb[size_t(lm) * w + i * 4];
+          for (uint32_t q = 0; q < 3; ++q) e[q] = uint32_t(t.mul_log(uint16_t(i << (5 * q)), uint16_t(lm))) * 0x10001u;
+          e[3] = uint32_t(t.mul_log(uint16_t(0x8000), uint16_t(lm))) * 0x10001u;
+        }
+      RS_CUDA(cudaMalloc(&f->d_kbank, kb.size() * 4));
+      RS_CUDA(cudaMemcpy(f->d_kbank, kb.data(), kb.size() * 4, cudaMemcpyHostToDevice));
       std::vector<uint32_t> sk(size_t(t.mod) * w);
-      for (uint32_t i = 0; i < t.mod; ++i) std::memcpy(&sk[size_t(i) * w], &bank[size_t(t.skew[i]) * w], w * 4);
+      for (uint32_t i = 0; i < t.mod; ++i) std::memcpy(&sk[size_t(i) * w], &kb[size_t(t.skew[i]) * w], w * 4);
       RS_CUDA(cudaMalloc(&f->d_sktab, sk.size() * 4));
       RS_CUDA(cudaMemcpy(f->d_sktab, sk.data(), sk.size() * 4, cudaMemcpyHostToDevice));
     }
