@@ -1075,7 +1075,7 @@ def serving_workload(args, torch, rsgpu, rank, gen):
     # (kernel loading, Leopard plans, pool growth) stay out of the latencies.
     # Every request rewrites only its own stripe from the same inputs, so
     # running them again leaves the arena unchanged.
-    srv = rsgpu.Server(device_budget=budget, streams=3, max_batch=512, planner="model")
+    srv = rsgpu.Server(device_budget=budget, streams=3, max_batch=64, planner="model")
     warm = min(256, len(specs))
     for i in range(warm):
         s = specs[i]
@@ -1085,7 +1085,7 @@ def serving_workload(args, torch, rsgpu, rank, gen):
     for load in args.serve_loads:
         lam = load * 1e9 / mean_bytes
         arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(specs)))
-        srv = rsgpu.Server(device_budget=budget, streams=3, max_batch=512, planner="model")
+        srv = rsgpu.Server(device_budget=budget, streams=3, max_batch=64, planner="model")
         comps = []
         t0 = time.perf_counter()
         for i, s in enumerate(specs):

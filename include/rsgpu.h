@@ -498,7 +498,7 @@ typedef struct rsgpu_server rsgpu_server;
 typedef struct rsgpu_server_options {
   size_t device_budget;  /* bytes admitted requests may hold (0: half of free memory) */
   uint32_t max_inflight; /* requests admitted at once (0: 4096) */
-  uint32_t max_batch;    /* requests per launch (0: 1024) */
+  uint32_t max_batch;    /* requests per launch (0: 64) */
   uint32_t streams;      /* launches in flight at once (0: 3) */
   int32_t planner;       /* RSGPU_PLANNER_* (default MODEL) */
 } rsgpu_server_options;

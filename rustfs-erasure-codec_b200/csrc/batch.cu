@@ -306,6 +306,10 @@ struct MixBatch {
   cudaGraphExec_t exec = nullptr;
   rsgpu_mix_info info{};
   std::vector<uint32_t *> owned_tables;  // private copies of classic decode tables
+  // One-shot batches: wide Leopard reconstructions run by their codec's own
+  // decode kernel, launched on the batch's stream after k_mix.
+  std::vector<std::shared_ptr<LeoLaunch>> side;
+  uint32_t mix_kernels = 0;  // k_mix launches per launch (0 or 1)
   // Stream-ordered batches (one-shot launches of the request server): device
   // memory comes from cudaMallocAsync on `stream` and goes back with
   // cudaFreeAsync after the work queued there, so neither building nor
@@ -341,6 +345,10 @@ struct MixBatch {
     if (args.n_items) {
       k_mix<<<grid, kMixThreads, smem, s>>>(args);
       RS_CUDA(cudaGetLastError());
+    }
+    for (const auto &L : side) {
+      const int rc = leo_launch(*L, s);
+      if (rc) return rc;
     }
     return RSGPU_OK;
   }
@@ -404,6 +412,23 @@ struct MixBuild {
     job_cost.push_back(cost);
   }
 };
+
+// Grows a stream's work-row buffer to `need` bytes (with headroom), in the
+// stream's order: the old buffer is freed behind the work queued before.
+cudaError_t grow_slot(ScratchSlot &slot, size_t need, cudaStream_t s) {
+  if (slot.bytes >= need) return cudaSuccess;
+  if (slot.ptr) {
+    cudaError_t e = cudaFreeAsync(slot.ptr, s);
+    if (e != cudaSuccess) return e;
+  }
+  slot.ptr = nullptr;
+  slot.bytes = 0;
+  const size_t want = need + need / 4;
+  cudaError_t e = cudaError_t(lib_malloc_async(&slot.ptr, want, s));
+  if (e != cudaSuccess) return e;
+  slot.bytes = want;
+  return cudaSuccess;
+}
 
 // Relative cost of one item: bytes it moves times a per-algorithm factor.
 // Only the order of the queue depends on it; the cost model refines it.
@@ -480,6 +505,24 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
     Codec &c = const_cast<rsgpu_codec *>(ops[i].codec)->c;
     if (!mix_plan_valid(c, ops[i].op, b.plans[i])) return RSGPU_ERR_INVALID_ARGUMENT;
   }
+  // One-shot batches (the request server's) route Leopard reconstructions
+  // whose k_mix work rows would not fit shared memory (GF(2^16) codes of
+  // 2048 lanes and more) to the codec's own decode kernel: one 1024-thread
+  // CTA per SM keeps a single work-row slab per SM in L2, where three k_mix
+  // CTAs per SM keep three.  Measured on a B200, GF(2^16) 2048+1024 at
+  // 8 KiB: 0.41 against 1.05 ms for one stripe, 3.08 against 5.03 ms for 16,
+  // 9.2 against 13.7 ms for 48 (k_mix at its fastest tile).  Encodes stay
+  // in k_mix: there the two are on par.  Same bytes either way.
+  std::vector<char> routed(n_ops, 0);
+  if (b.stream_ordered)
+    for (size_t i = 0; i < n_ops; ++i) {
+      Codec &c = const_cast<rsgpu_codec *>(ops[i].codec)->c;
+      if (!is_leopard(c) || ops[i].op != RSGPU_OP_RECONSTRUCT || b.plans[i].algo != RSGPU_ALGO_FFT) continue;
+      LeoGeometry g{};
+      int rc = leopard_geometry(c, &g);
+      if (rc) return rc;
+      routed[i] = size_t(fft_rows(g, ops[i].op)) * 2 * 64 > kMixSmem;
+    }
 
   MixBuild B;
   // Decode tables and locators are built on the batch's stream when it has
@@ -492,7 +535,7 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   std::map<const Codec *, std::vector<size_t>> leo_fft_rec;
   for (size_t i = 0; i < n_ops; ++i) {
     const Codec &c = ops[i].codec->c;
-    if (ops[i].op != RSGPU_OP_RECONSTRUCT) continue;
+    if (ops[i].op != RSGPU_OP_RECONSTRUCT || routed[i]) continue;
     if (!is_leopard(c))
       classic_rec[&c].push_back(i);
     else if (b.plans[i].algo == RSGPU_ALGO_APPLY)
@@ -602,8 +645,46 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
     dense_enc_tbl[&c] = off;
   }
 
+  // ---- routed reconstructions: one launch per (codec, shard length, goal).
+  // Their work rows go to the stream's own buffer (the caller's ScratchSlot,
+  // shared with k_mix's wide tiles, which run before them on the stream),
+  // sized below for the larger of the two users.
+  size_t routed_scratch = 0;
+  {
+    std::map<std::tuple<const Codec *, size_t, int>, std::vector<size_t>> groups;
+    for (size_t i = 0; i < n_ops; ++i)
+      if (routed[i]) groups[std::make_tuple(&ops[i].codec->c, ops[i].shard_len, ops[i].goal)].push_back(i);
+    for (auto &kv : groups) {
+      Codec &c = const_cast<Codec &>(*std::get<0>(kv.first));
+      const size_t total = c.k + c.m, len = std::get<1>(kv.first);
+      std::vector<uint8_t *> sh;
+      std::vector<uint8_t> pres;
+      for (size_t i : kv.second) {
+        sh.insert(sh.end(), ops[i].shards, ops[i].shards + total);
+        pres.insert(pres.end(), ops[i].present, ops[i].present + total);
+        size_t np = 0, nt = 0;
+        for (size_t x = 0; x < total; ++x) {
+          np += ops[i].present[x] ? 1 : 0;
+          nt += !ops[i].present[x] && (ops[i].goal == RSGPU_GOAL_ALL || x < c.k);
+        }
+        if (nt) B.algorithmic_bytes += uint64_t(np + nt) * len;
+      }
+      std::shared_ptr<LeoLaunch> L;
+      const size_t want = scratch ? leo_reconstruct_scratch_bytes(c) : 0;
+      if (want) {
+        RS_CUDA(grow_slot(*scratch, want, b.stream));
+        routed_scratch = std::max(routed_scratch, want);
+      }
+      int rc = prepare_leo_reconstruct_once(c, kv.second.size(), sh.data(), pres.data(), len, std::get<2>(kv.first),
+                                            b.stream, want ? scratch->ptr : nullptr, L);
+      if (rc) return rc;
+      b.side.push_back(L);
+    }
+  }
+
   // ---- jobs
   for (size_t i = 0; i < n_ops; ++i) {
+    if (routed[i]) continue;
     const rsgpu_mix_op &o = ops[i];
     Codec &c = const_cast<rsgpu_codec *>(o.codec)->c;
     const size_t total = c.k + c.m, len = o.shard_len;
@@ -825,19 +906,13 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   per_sm = std::max(per_sm, 1);
   if (opt.ctas_per_sm > 0) per_sm = std::min(per_sm, int(opt.ctas_per_sm));
   b.grid = int(std::max<uint64_t>(1, std::min<uint64_t>(items.size(), uint64_t(per_sm) * sm_count())));
-  if (B.scratch_words) {
-    const size_t need = size_t(b.grid) * B.scratch_words * 4;
+  if (B.scratch_words || routed_scratch) {
+    const size_t need = std::max(size_t(b.grid) * B.scratch_words * 4, routed_scratch);
     if (scratch && b.stream_ordered) {
-      if (scratch->bytes < need) {  // grow with headroom, in the stream's order
-        if (scratch->ptr) RS_CUDA(cudaFreeAsync(scratch->ptr, b.stream));
-        scratch->ptr = nullptr;
-        scratch->bytes = 0;
-        const size_t want = need + need / 4;
-        RS_CUDA(cudaError_t(lib_malloc_async(&scratch->ptr, want, b.stream)));
-        scratch->bytes = want;
-      }
+      RS_CUDA(grow_slot(*scratch, need, b.stream));
       b.d_scratch = static_cast<uint32_t *>(scratch->ptr);
       b.scratch_borrowed = true;
+      for (const auto &L : b.side) leo_set_scratch(*L, scratch->ptr);  // the buffer may have moved
     } else {
       RS_CUDA(b.alloc(&b.d_scratch, need));
     }
@@ -861,7 +936,9 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   b.info.smem_bytes = uint32_t(b.smem);
   b.info.device_bytes = total_bytes + size_t(b.grid) * B.scratch_words * 4;
   b.info.algorithmic_bytes = B.algorithmic_bytes;
-  b.info.kernels_per_launch = items.empty() ? 0 : 1;
+  b.mix_kernels = items.empty() ? 0 : 1;
+  b.info.kernels_per_launch = b.mix_kernels;
+  for (const auto &L : b.side) b.info.kernels_per_launch += leo_kernel_count(*L);
 
   if (opt.graph) {
     cudaStream_t cs = nullptr;
@@ -888,7 +965,7 @@ int mix_launch(MixBatch &b, cudaStream_t s) {
     int rc = b.enqueue(s);
     if (rc) return rc;
   }
-  launch_counter_add(b.info.kernels_per_launch);
+  launch_counter_add(b.mix_kernels);  // the routed launches count themselves
   return RSGPU_OK;
 }
 

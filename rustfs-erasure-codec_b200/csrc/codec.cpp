@@ -137,6 +137,25 @@ int upload_to(void *dst, const void *src, size_t bytes, void *stream) {
   return RSGPU_OK;
 }
 
+// Gives the calling thread's bounce-buffer pool at least `n` free buffers of
+// `bytes` each, so that its first uploads of up to that size allocate no
+// pinned memory (cudaHostAlloc of megabytes took tens of milliseconds on a
+// request path).
+int upload_prewarm(size_t n, size_t bytes) {
+  UploadPool &pool = t_upload;
+  size_t have = 0;
+  for (auto &x : pool.slots) have += x->cap >= bytes ? 1 : 0;
+  while (have < n && pool.slots.size() < kUploadSlots) {
+    pool.slots.emplace_back(new UploadSlot());
+    UploadSlot *u = pool.slots.back().get();
+    RS_CUDA(cudaEventCreateWithFlags(&u->done, cudaEventDisableTiming));
+    RS_CUDA(cudaHostAlloc(&u->host, bytes, cudaHostAllocDefault));
+    u->cap = bytes;
+    ++have;
+  }
+  return RSGPU_OK;
+}
+
 namespace {
 // Copies `bytes` of host data to a fresh stream-ordered device allocation
 // (upload_to).  The device block is freed stream-ordered by the caller.

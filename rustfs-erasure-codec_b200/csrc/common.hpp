@@ -64,5 +64,7 @@ int lib_pool(void **out);
 // buffer of the calling thread (never blocks on the stream's earlier work).
 // Returns an RSGPU_* code.
 int upload_to(void *dst, const void *src, size_t bytes, void *stream);
+// At least n free bounce buffers of `bytes` in the calling thread's pool.
+int upload_prewarm(size_t n, size_t bytes);
 
 }  // namespace rsgpu

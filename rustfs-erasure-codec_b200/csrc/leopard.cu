@@ -481,6 +481,10 @@ struct LeoLaunch {
   int grid = 0;
   size_t smem = 0;
   bool global_work = false;
+  // Work rows in a caller-owned buffer private to the launch's stream
+  // (instead of the codec's shared slab, which launches on different streams
+  // take in turn).
+  void *own_scratch = nullptr;
   ~LeoLaunch() {
     if (!d_blob) return;
     if (blob_ordered)
@@ -667,6 +671,10 @@ int configure_fft(const K kernel, const K2 kernel_wide, LeoLaunch &L, uint32_t r
     L.threads = kWideThreads;
     L.grid = int(std::min<uint64_t>(tiles, uint64_t(kGlobalBlocks) * sm_count()));
     const size_t need = size_t(L.grid) * rows * nb * 64;
+    if (L.own_scratch) {  // sized by the caller for a full grid
+      L.args.scratch = static_cast<uint32_t *>(L.own_scratch);
+      return RSGPU_OK;
+    }
     int rc = grow_scratch(st, need);
     if (rc) return rc;
     {
@@ -1040,7 +1048,7 @@ int leo_launch_kernel(const LeoLaunch &L, cudaStream_t s);
 // capture cannot be waited on inside it).
 int leo_launch(const LeoLaunch &L, cudaStream_t s) {
   if (L.args.n_jobs == 0) return RSGPU_OK;
-  if (!L.global_work) return leo_launch_kernel(L, s);
+  if (!L.global_work || L.own_scratch) return leo_launch_kernel(L, s);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   RS_CUDA(cudaStreamIsCapturing(s, &cap));
   if (cap != cudaStreamCaptureStatusNone) return leo_launch_kernel(L, s);
@@ -1124,6 +1132,30 @@ int prepare_other(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, co
   if (c.family == RSGPU_FAMILY_CLASSIC) return prepare_tower(c, op, n_stripes, shards, present, len, goal, flags, out);
   auto L = std::make_shared<LeoLaunch>();
   int rc = build_leo(c, op, n_stripes, shards, present, len, goal, nullptr, 0, flags, *L, nullptr, false);
+  if (rc) return rc;
+  out = L;
+  return RSGPU_OK;
+}
+
+// Work rows of a full grid of the decode kernel when they live in global
+// memory (configure_fft: n rows of two 64-byte blocks per CTA, beyond
+// 200 KiB of shared memory); 0 when they fit shared memory.
+size_t leo_reconstruct_scratch_bytes(Codec &c) {
+  const size_t rows = c.leo->n, per_cta = rows * 2 * 64;
+  return per_cta > 200 * 1024 ? size_t(kGlobalBlocks) * sm_count() * per_cta : 0;
+}
+
+void leo_set_scratch(LeoLaunch &L, void *scratch) {
+  if (!L.own_scratch) return;
+  L.own_scratch = scratch;
+  L.args.scratch = static_cast<uint32_t *>(scratch);
+}
+
+int prepare_leo_reconstruct_once(Codec &c, size_t n, uint8_t *const *shards, const uint8_t *present, size_t len,
+                                 int goal, cudaStream_t s, void *scratch, std::shared_ptr<LeoLaunch> &out) {
+  auto L = std::make_shared<LeoLaunch>();
+  L->own_scratch = leo_reconstruct_scratch_bytes(c) ? scratch : nullptr;
+  int rc = build_leo(c, RSGPU_OP_RECONSTRUCT, n, shards, present, len, goal, nullptr, 0, nullptr, *L, s, true);
   if (rc) return rc;
   out = L;
   return RSGPU_OK;

@@ -22,6 +22,20 @@ struct LeoLaunch;
 int prepare_other(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
                   int goal, uint32_t *flags, std::shared_ptr<LeoLaunch> &out);
 int leo_launch(const LeoLaunch &l, cudaStream_t s);
+// A one-shot Leopard reconstruction of n stripes of one codec, shard length
+// and goal through the codec's own decode kernel, built on stream s: its job
+// blob is allocated on s and freed there, behind the kernel, when the launch
+// is destroyed, and building it never waits for the device (a codec's first
+// wide decode may grow its work-row slab with cudaMalloc).
+// With `scratch` (a device buffer private to stream s, at least
+// leo_reconstruct_scratch_bytes(c) bytes) the launch keeps its work rows
+// there instead of in the codec's shared slab, so it neither grows that slab
+// nor waits for other streams' launches that use it; leo_set_scratch moves it
+// to another such buffer before the launch.
+int prepare_leo_reconstruct_once(Codec &c, size_t n, uint8_t *const *shards, const uint8_t *present, size_t len,
+                                 int goal, cudaStream_t s, void *scratch, std::shared_ptr<LeoLaunch> &out);
+size_t leo_reconstruct_scratch_bytes(Codec &c);
+void leo_set_scratch(LeoLaunch &l, void *scratch);
 int prepare_tower(Codec &c, int op, size_t n_stripes, uint8_t *const *shards, const uint8_t *present, size_t len,
                   int goal, uint32_t *flags, std::shared_ptr<LeoLaunch> &out);
 uint32_t leo_kernel_count(const LeoLaunch &l);

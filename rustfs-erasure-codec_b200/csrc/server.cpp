@@ -39,6 +39,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <future>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -129,7 +130,12 @@ class Server {
       opt_.device_budget = free_b / 2;
     }
     if (opt_.max_inflight == 0) opt_.max_inflight = 4096;
-    if (opt_.max_batch == 0) opt_.max_batch = 1024;
+    // 64 requests per launch: on the bench's serving stream at 800 GB/s
+    // offered (B200), 64 gave 334-346 GB/s with p50 42-47 ms and p99 75-81 ms,
+    // 512 gave 326-344 GB/s with p50 60-64 ms and p99 85-100 ms (32: as 64,
+    // with more host time per byte).  Smaller launches let the streams
+    // overlap and shorten the last launch of a burst.
+    if (opt_.max_batch == 0) opt_.max_batch = 64;
     if (opt_.streams == 0) opt_.streams = 3;
     flights_.resize(opt_.streams);
     for (auto &f : flights_) {
@@ -156,8 +162,33 @@ class Server {
         cudaGetLastError();  // an out-of-memory here is not sticky
       }
     }
+    // Memory the first batches would otherwise map on a request's path:
+    // growing the library's device pool (work rows, batch blobs) mapped fresh
+    // device memory for 15-100 ms in the first batches of a server.  A block
+    // allocated and freed here stays in the pool, which keeps up to 2 GiB of
+    // freed memory.  Best effort, like the buffers above.
+    {
+      void *p = nullptr;
+      if (cudaError_t(lib_malloc_async(&p, kPoolReserve, flights_[0].stream)) == cudaSuccess) {
+        cudaFreeAsync(p, flights_[0].stream);
+        cudaStreamSynchronize(flights_[0].stream);
+      } else {
+        cudaGetLastError();
+      }
+    }
     t0_ = Clock::now();
-    worker_ = std::thread([this] { loop(); });
+    // The worker's bounce buffers (batch blobs go through them) are
+    // allocated before start returns: cudaHostAlloc of tens of megabytes at
+    // the top of the loop delayed a new server's first requests by ~30 ms.
+    std::promise<void> warm;
+    std::future<void> warmed = warm.get_future();
+    worker_ = std::thread([this, &warm] {
+      cudaSetDevice(device_);
+      upload_prewarm(kUploadWarmBuffers, kUploadWarmBytes);
+      warm.set_value();
+      loop();
+    });
+    warmed.wait();
     return RSGPU_OK;
   }
 
@@ -249,6 +280,9 @@ class Server {
   }
 
  private:
+  static constexpr size_t kPoolReserve = size_t(1) << 30;
+  static constexpr size_t kUploadWarmBuffers = 4;
+  static constexpr size_t kUploadWarmBytes = size_t(16) << 20;
   rsgpu_server_options opt_;
   int device_ = 0;
   std::thread worker_;
@@ -520,7 +554,6 @@ class Server {
   }
 
   void loop() {
-    cudaSetDevice(device_);
     double last = now();
     for (;;) {
       const double t_pass = now();

@@ -226,3 +226,36 @@ def test_repeated_leopard_pattern_fft_then_dense_map(rs, torch, codecs):
         srv.close()
     finally:
         rs.Tuner.clear()
+
+
+def test_wide_leopard_decodes_run_by_the_codec_kernel(rs, torch):
+    # Leopard GF(2^16) reconstructions whose work rows do not fit k_mix's
+    # shared memory (here 1024 and 2048 lanes) leave the server's mixed batch
+    # for their codec's own decode kernel on the batch's stream.  Their bytes
+    # must equal the oracle's, alone and in batches that mix them with
+    # encodes, classic rebuilds and each other (goals all and data).
+    geoms = [("leopard_gf16", 300, 100), ("leopard_gf16", 1024, 512), ("classic", 10, 4)]
+    cods = {g: rs.ReedSolomon(g[1], g[2], rs.CodecOptions(codec_family=g[0])) for g in geoms}
+    rng = np.random.default_rng(77)
+    reqs = []
+    for i in range(30):
+        g = geoms[i % 3]
+        fam, k, m = g
+        op = "reconstruct" if i % 5 else "encode"
+        length = int(rng.integers(1, 4)) * 64
+        data = rng.integers(0, 256, (k + m, length), dtype=np.uint8)
+        present, goal = None, "all"
+        if op == "reconstruct":
+            e = int(rng.integers(1, m + 1))
+            present = np.ones(k + m, np.uint8)
+            present[rng.choice(k + m, size=e, replace=False)] = 0
+            goal = "data" if i % 4 == 0 else "all"
+        reqs.append(dict(geom=g, op=op, data=data, present=present, goal=goal, len=length))
+    srv = rs.Server(streams=3, max_batch=8)
+    alone, _, _ = run(rs, srv, cods, reqs, one_at_a_time=True, device=torch)
+    mixed, _, _ = run(rs, srv, cods, reqs, one_at_a_time=False, device=torch)
+    srv.close()
+    for i, r in enumerate(reqs):
+        want, _ = oracle_apply(r["geom"], cods[r["geom"]], r["op"], r["data"], r["present"], r["goal"])
+        assert np.array_equal(alone[i], want), (i, r["geom"], r["op"], r["goal"])
+        assert np.array_equal(mixed[i], want), (i, r["geom"], r["op"], r["goal"])
