@@ -310,6 +310,7 @@ struct MixBatch {
   // decode kernel, launched on the batch's stream after k_mix.
   std::vector<std::shared_ptr<LeoLaunch>> side;
   uint32_t mix_kernels = 0;  // k_mix launches per launch (0 or 1)
+  std::vector<void *> ordered_bufs;  // one-shot batches: dense maps derived on the stream
   // Stream-ordered batches (one-shot launches of the request server): device
   // memory comes from cudaMallocAsync on `stream` and goes back with
   // cudaFreeAsync after the work queued there, so neither building nor
@@ -322,6 +323,7 @@ struct MixBatch {
     if (stream_ordered) {
       for (void *p : {(void *)d_blob, (void *)d_flags, (void *)d_counter, (void *)d_locs})
         if (p) cudaFreeAsync(p, stream);
+      for (void *p : ordered_bufs) cudaFreeAsync(p, stream);
       if (d_scratch && !scratch_borrowed) cudaFreeAsync(d_scratch, stream);
       return;
     }
@@ -523,6 +525,23 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
       if (rc) return rc;
       routed[i] = size_t(fft_rows(g, ops[i].op)) * 2 * 64 > kMixSmem;
     }
+  // One-shot batches run large Leopard GF(2^8) rebuilds whose dense map is
+  // not cached through a map derived on the batch's stream (the FFT decode
+  // of unit vectors, then a packing kernel; no host wait) instead of the FFT
+  // decode.  One B200, one stripe of 4 MiB shards, k_mix: 128+64 rebuilds in
+  // 1.53 ms through the map against 4.95 ms by the FFT (5.14 ms by the
+  // codec's decode kernel), 32+16 in 0.12 against 1.02 ms; deriving costs
+  // two small launches.  Same bytes: the map is the decode's own.
+  constexpr uint64_t kInlineDenseBytes = uint64_t(32) << 20;
+  std::vector<char> inline_dense(n_ops, 0);
+  if (b.stream_ordered)
+    for (size_t i = 0; i < n_ops; ++i) {
+      Codec &c = const_cast<rsgpu_codec *>(ops[i].codec)->c;
+      if (c.family != RSGPU_FAMILY_LEOPARD_GF8 || ops[i].op != RSGPU_OP_RECONSTRUCT ||
+          b.plans[i].algo != RSGPU_ALGO_FFT || routed[i])
+        continue;
+      inline_dense[i] = uint64_t(c.k + c.m) * ops[i].shard_len >= kInlineDenseBytes;
+    }
 
   MixBuild B;
   // Decode tables and locators are built on the batch's stream when it has
@@ -535,7 +554,7 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   std::map<const Codec *, std::vector<size_t>> leo_fft_rec;
   for (size_t i = 0; i < n_ops; ++i) {
     const Codec &c = ops[i].codec->c;
-    if (ops[i].op != RSGPU_OP_RECONSTRUCT || routed[i]) continue;
+    if (ops[i].op != RSGPU_OP_RECONSTRUCT || routed[i] || inline_dense[i]) continue;
     if (!is_leopard(c))
       classic_rec[&c].push_back(i);
     else if (b.plans[i].algo == RSGPU_ALGO_APPLY)
@@ -645,6 +664,33 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
     dense_enc_tbl[&c] = off;
   }
 
+  // ---- inline dense maps (one-shot batches): derived on the stream now
+  struct InlineMap {
+    std::vector<uint16_t> inputs, targets;
+    const uint32_t *tbl = nullptr;
+  };
+  std::vector<InlineMap> imaps(n_ops);
+  for (size_t i = 0; i < n_ops; ++i) {
+    if (!inline_dense[i]) continue;
+    Codec &c = const_cast<rsgpu_codec *>(ops[i].codec)->c;
+    uint8_t *img = nullptr;
+    RS_CUDA(b.alloc(&img, leopard_dense_inline_bytes(c, ops[i].present, ops[i].goal)));
+    b.ordered_bufs.push_back(img);
+    size_t nt = 0, ni = 0;
+    for (size_t x = 0; x < c.k + c.m; ++x) {
+      ni += ops[i].present[x] ? 1 : 0;
+      nt += !ops[i].present[x] && (ops[i].goal == RSGPU_GOAL_ALL || x < c.k);
+    }
+    uint32_t *tbl = nullptr;
+    RS_CUDA(b.alloc(&tbl, std::max<size_t>(packed_table_words(nt, ni), 1) * 4));
+    b.ordered_bufs.push_back(tbl);
+    int rc = leopard_dense_inline(c, ops[i].present, ops[i].goal, img, tbl, imaps[i].inputs, imaps[i].targets,
+                                  b.stream);
+    if (rc) return rc;
+    imaps[i].tbl = tbl;
+    b.plans[i] = rsgpu_plan{RSGPU_ALGO_APPLY, imaps[i].targets.size() > 4 ? 2 : 0};
+  }
+
   // ---- routed reconstructions: one launch per (codec, shard length, goal).
   // Their work rows go to the stream's own buffer (the caller's ScratchSlot,
   // shared with k_mix's wide tiles, which run before them on the stream),
@@ -686,6 +732,16 @@ int mix_build(const rsgpu_mix_op *ops, size_t n_ops, const rsgpu_plan *forced, c
   for (size_t i = 0; i < n_ops; ++i) {
     if (routed[i]) continue;
     const rsgpu_mix_op &o = ops[i];
+    if (inline_dense[i]) {
+      const InlineMap &mp = imaps[i];
+      if (mp.targets.empty()) continue;
+      const size_t off = B.ptrs.size();
+      for (uint16_t x : mp.inputs) B.ptrs.push_back(o.shards[x]);
+      for (uint16_t t : mp.targets) B.ptrs.push_back(o.shards[t]);
+      add_apply_job(B, b.plans[i], false, mp.inputs.size(), mp.targets.size(), off, o.shard_len, 0, mp.tbl, SIZE_MAX);
+      B.algorithmic_bytes += uint64_t(mp.inputs.size() + mp.targets.size()) * o.shard_len;
+      continue;
+    }
     Codec &c = const_cast<rsgpu_codec *>(o.codec)->c;
     const size_t total = c.k + c.m, len = o.shard_len;
     const rsgpu_plan &p = b.plans[i];

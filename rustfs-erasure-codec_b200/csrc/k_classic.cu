@@ -509,7 +509,8 @@ cudaError_t launch_apply(const ApplyArgs &a, bool verify, uint64_t max_tail, cud
     const uint64_t n = max_tail * a.n_jobs;
     const int threads = 256;
     const uint64_t want = (n + threads - 1) / threads;
-    const int grid = int(want < 148 * 16 ? want : 148 * 16);
+    const uint64_t cap = uint64_t(device_sm_count()) * 16;
+    const int grid = int(want < cap ? want : cap);
     if (a.accumulate)
       k_apply_tail<false, true><<<grid, threads, 0, s>>>(a, max_tail);
     else if (verify)

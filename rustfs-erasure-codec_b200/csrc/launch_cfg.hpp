@@ -14,6 +14,21 @@
 
 namespace rsgpu {
 
+// SMs of the current device (queried once per device).
+inline int device_sm_count() {
+  static std::mutex mu;
+  static std::map<int, int> sms;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = sms.find(dev);
+  if (it != sms.end()) return it->second;
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 1;
+  sms[dev] = n;
+  return n;
+}
+
 // Makes `fn` launchable with `smem` bytes of dynamic shared memory.
 inline cudaError_t ensure_smem_limit(const void *fn, size_t smem) {
   if (smem <= 48 * 1024) return cudaSuccess;

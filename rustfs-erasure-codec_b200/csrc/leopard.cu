@@ -149,6 +149,7 @@ struct LeoField {
   uint32_t *d_bank = nullptr;   // multiplier tables indexed by log value (half-warp layer kernels)
   uint32_t *d_kbank = nullptr;  // tables of the register-stage kernels (GF(2^8): 5+3 split; GF(2^16): 5+5+5+1)
   uint32_t *d_sktab = nullptr;  // d_kbank's entry of each skew entry: entry i holds the tables of log skew[i]
+  uint8_t *d_mul8 = nullptr;    // GF(2^8): products mul[a][b], 256 x 256 (device packing of dense maps)
   explicit LeoField(int b) : bits(b), host(b) {}
 };
 
@@ -205,6 +206,11 @@ static int leo_field(int bits, LeoField **out) {
         std::memcpy(&sk[size_t(i) * kWBank8], &kb[size_t(t.skew[i]) * kWBank8], kWBank8 * 4);
       RS_CUDA(cudaMalloc(&f->d_sktab, sk.size() * 4));
       RS_CUDA(cudaMemcpy(f->d_sktab, sk.data(), sk.size() * 4, cudaMemcpyHostToDevice));
+      std::vector<uint8_t> mul(256 * 256, 0);
+      for (uint32_t a = 1; a < 256; ++a)
+        for (uint32_t b = 1; b < 256; ++b) mul[a * 256 + b] = uint8_t(t.exp[t.add_mod(t.log[a], t.log[b])]);
+      RS_CUDA(cudaMalloc(&f->d_mul8, mul.size()));
+      RS_CUDA(cudaMemcpy(f->d_mul8, mul.data(), mul.size(), cudaMemcpyHostToDevice));
     } else {
       // Per log value, 32 lanes x 4 words (layout of leo_fft.cuh): c * i,
       // c * (i << 5), c * (i << 10) for i = lane, and c * 2^15, each
@@ -1701,6 +1707,82 @@ int leopard_dense_derive_finish(DenseDerivation &d) {
   std::lock_guard<std::mutex> g(st.mu);
   dense_insert_locked(st, d.pattern + char(d.goal), std::move(maps[0]));
   return RSGPU_OK;
+}
+
+// ---------------------------------------------------------------- dense maps derived in stream order
+namespace {
+
+// Packs the K1 tables of one dense map on the device, in the layout of
+// pack_tables_with (common.hpp: kTableWords words per group of four targets
+// and input), from the decoded unit-vector stripe: coefficient (t, q) is
+// byte q of shard targets[t].  One thread per table word.
+__global__ void __launch_bounds__(256) k_pack_dense8(const uint8_t *units, uint32_t L, const uint16_t *targets,
+                                                     uint32_t nt, uint32_t ni, const uint8_t *mul, uint32_t *out) {
+  const uint32_t groups = (nt + 3) / 4;
+  const uint64_t total = uint64_t(groups) * ni * kTableWords;
+  for (uint64_t x = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; x < total; x += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t w = uint32_t(x % kTableWords);
+    const uint64_t gj = x / kTableWords;
+    const uint32_t j = uint32_t(gj % ni), g = uint32_t(gj / ni);
+    uint32_t word = 0;
+    for (uint32_t r = 0; r < 4; ++r) {
+      const uint32_t o = g * 4 + r;
+      if (o >= nt) break;
+      const uint8_t *row = mul + uint32_t(units[size_t(targets[o]) * L + j]) * 256;
+      if (w < 16)
+        word |= uint32_t(row[w]) << (8 * r);
+      else if (w < 32)
+        word |= uint32_t(row[(w - 16) << 4]) << (8 * r);
+      else if (w < 64)
+        word |= uint32_t(row[w - 32]) << (8 * r);
+      else if (((w - 64) >> 1) == r) {
+        const uint32_t h0 = 4 * ((w - 64) & 1);
+        for (uint32_t b = 0; b < 4; ++b) word |= uint32_t(row[(h0 + b) << 5]) << (8 * b);
+      }
+    }
+    out[x] = word;
+  }
+}
+
+}  // namespace
+
+// Bytes of the device image leopard_dense_inline works in: the unit-vector
+// stripe (k + m shards of L = the inputs rounded up to 64 bytes) and the
+// target list.
+size_t leopard_dense_inline_bytes(Codec &c, const uint8_t *present, int goal) {
+  std::vector<LeoDenseMap> maps;
+  const size_t L = dense_layout(c, 1, present, goal, maps);
+  return (c.k + c.m) * L + ((maps[0].targets.size() * 2 + 15) & ~size_t(15)) + 16;
+}
+
+int leopard_dense_inline(Codec &c, const uint8_t *present, int goal, uint8_t *d_img, uint32_t *d_tbl,
+                         std::vector<uint16_t> &inputs, std::vector<uint16_t> &targets, cudaStream_t s) {
+  LeopardState &st = *c.leo;
+  if (st.field->bits != 8) return RSGPU_ERR_INVALID_ARGUMENT;
+  const size_t total = c.k + c.m;
+  std::vector<LeoDenseMap> maps;
+  const size_t L = dense_layout(c, 1, present, goal, maps);
+  inputs = maps[0].inputs;
+  targets = maps[0].targets;
+  if (targets.empty()) return RSGPU_OK;
+  const size_t units = total * L;
+  std::vector<uint8_t> host(leopard_dense_inline_bytes(c, present, goal), 0);
+  dense_units(c, maps, L, host.data());
+  std::memcpy(host.data() + units, targets.data(), targets.size() * 2);
+  int rc = upload_to(d_img, host.data(), host.size(), s);
+  if (rc) return rc;
+  std::vector<uint8_t *> ptrs(total);
+  for (size_t i = 0; i < total; ++i) ptrs[i] = d_img + i * L;
+  // The FFT decode of the unit vectors (the pattern's own transform), then
+  // the packing, both queued on s ahead of the batch that applies the map.
+  rc = run_once(c, RSGPU_OP_RECONSTRUCT, 1, ptrs.data(), present, L, goal, nullptr, 0, nullptr, s);
+  if (rc) return rc;
+  const uint64_t words = packed_table_words(targets.size(), inputs.size());
+  const int grid = int(std::min<uint64_t>((words + 255) / 256, uint64_t(sm_count()) * 8));
+  k_pack_dense8<<<grid, 256, 0, s>>>(d_img, uint32_t(L), reinterpret_cast<const uint16_t *>(d_img + units),
+                                     uint32_t(targets.size()), uint32_t(inputs.size()), st.field->d_mul8, d_tbl);
+  launch_counter_add(1);
+  return cuda_status(cudaGetLastError());
 }
 
 // ====================================================================== no allocation

@@ -103,6 +103,15 @@ int leopard_dense_decode(Codec &c, size_t n, const uint8_t *present, int goal, s
 bool leopard_dense_due(Codec &c, const uint8_t *present, int goal, size_t len);
 // Whether the codec's map cache holds this pattern's map.
 bool leopard_dense_cached(Codec &c, const uint8_t *present, int goal);
+// A GF(2^8) reconstruction's dense map derived and packed on the device, all
+// queued on stream s (no host wait): d_img (leopard_dense_inline_bytes bytes)
+// holds the unit-vector stripe the pattern's FFT decode runs on, d_tbl
+// (packed_table_words(targets, inputs) words) receives the K1 tables.  Both
+// buffers must stay allocated until the work queued on s has run.  Returns
+// the map's inputs and targets (ascending shard indices); no targets, no work.
+size_t leopard_dense_inline_bytes(Codec &c, const uint8_t *present, int goal);
+int leopard_dense_inline(Codec &c, const uint8_t *present, int goal, uint8_t *d_img, uint32_t *d_tbl,
+                         std::vector<uint16_t> &inputs, std::vector<uint16_t> &targets, cudaStream_t s);
 
 // A map derived off the request path: start queues the FFT decode of the
 // pattern's unit vectors on stream s through a caller-owned pinned buffer of

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "codec.hpp"
+#include "launch_cfg.hpp"
 #include "leopard.hpp"
 
 namespace rsgpu {
@@ -203,7 +204,7 @@ static int launch_tower(const std::vector<JobDesc> &jobs, const std::vector<cons
   a.n_jobs = uint32_t(js.size());
   a.accumulate = accumulate ? 1 : 0;
   const uint64_t tiles = ((len + 4095) / 4096) * js.size();
-  const int grid = int(std::min<uint64_t>(tiles, 148 * 8));
+  const int grid = int(std::min<uint64_t>(tiles, uint64_t(device_sm_count()) * 8));
   if (verify)
     k_apply_tower<true><<<grid, 256, 0, s>>>(a);
   else

@@ -259,3 +259,33 @@ def test_wide_leopard_decodes_run_by_the_codec_kernel(rs, torch):
         want, _ = oracle_apply(r["geom"], cods[r["geom"]], r["op"], r["data"], r["present"], r["goal"])
         assert np.array_equal(alone[i], want), (i, r["geom"], r["op"], r["goal"])
         assert np.array_equal(mixed[i], want), (i, r["geom"], r["op"], r["goal"])
+
+
+def test_large_leopard_gf8_rebuilds_through_maps_derived_on_the_stream(rs, torch):
+    # Leopard GF(2^8) rebuilds of 32 MiB stripes and more whose dense map is
+    # not cached run, in the server's batches, through a map derived on the
+    # batch's stream (FFT decode of unit vectors, then device packing).  Every
+    # fresh pattern must give the oracle's bytes, goals all and data, in
+    # batches alone and together with other requests.
+    geoms = [("leopard_gf8", 32, 16), ("leopard_gf8", 128, 64), ("classic", 10, 4)]
+    cods = {g: rs.ReedSolomon(g[1], g[2], rs.CodecOptions(codec_family=g[0])) for g in geoms}
+    rng = np.random.default_rng(91)
+    reqs = []
+    for i in range(9):
+        g = geoms[i % 3]
+        fam, k, m = g
+        length = (1 << 20) if g[1] == 32 else (256 << 10) if g[1] == 128 else (64 << 10)
+        data = rng.integers(0, 256, (k + m, length), dtype=np.uint8)
+        e = int(rng.integers(1, m + 1))
+        present = np.ones(k + m, np.uint8)
+        present[rng.choice(k + m, size=e, replace=False)] = 0
+        goal = "data" if i % 4 == 1 else "all"
+        reqs.append(dict(geom=g, op="reconstruct", data=data, present=present, goal=goal, len=length))
+    srv = rs.Server(streams=2, max_batch=4)
+    alone, _, _ = run(rs, srv, cods, reqs, one_at_a_time=True, device=torch)
+    mixed, _, _ = run(rs, srv, cods, reqs, one_at_a_time=False, device=torch)
+    srv.close()
+    for i, r in enumerate(reqs):
+        want, _ = oracle_apply(r["geom"], cods[r["geom"]], r["op"], r["data"], r["present"], r["goal"])
+        assert np.array_equal(alone[i], want), (i, r["geom"], r["goal"])
+        assert np.array_equal(mixed[i], want), (i, r["geom"], r["goal"])
