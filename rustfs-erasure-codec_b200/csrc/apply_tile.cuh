@@ -66,9 +66,13 @@ __device__ __forceinline__ void mac4_lo5(uint32_t w, uint32_t t5, uint32_t *a) {
 }
 
 // 5+3 split, PRMT half: selector nibble c = high three bits of byte c of w.
+// y = x | (x >> 4) puts byte i + 1's field in the high nibble of byte i; the
+// fields do not overlap, so it equals x + (x >> 4), which one multiply-high
+// and add computes on the FMA pipe (the GF(2^8) transforms are bound by the
+// integer pipe).
 __device__ __forceinline__ uint32_t hi3_selector(uint32_t w) {
   const uint32_t x = (w >> 5) & 0x07070707u;
-  const uint32_t y = x | ((w >> 9) & 0x00707070u);
+  const uint32_t y = __umulhi(x, 1u << 28) + x;
   return __byte_perm(y, 0, 0x3320);
 }
 
