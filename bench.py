@@ -760,6 +760,27 @@ def config1_workload(torch, rsgpu, stream, gen):
         out[name] = {"us": round(med * 1e3, 1), "p99_us": round(p99 * 1e3, 1),
                      "gbs": round(nbytes / (med / 1e3) / 1e9, 1),
                      "data_gibs": round(n * k * size / (med / 1e3) / 2**30, 1)}
+    # One step (encode, rebuild, verify) as one CUDA graph of the three
+    # prepared launches, so no host launch latency sits between them (the
+    # per-operation times above include it: each launch starts on an idle
+    # stream).
+    try:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            enc.launch()
+            rec.launch()
+            ver.launch()
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+        med, p99 = _median_ms(torch, stream, g.replay, 20)
+        out["step_graph"] = {"ops": "encode + reconstruct + verify, one CUDA graph",
+                             "us": round(med * 1e3, 1), "p99_us": round(p99 * 1e3, 1),
+                             "gbs": round(3 * nbytes / (med / 1e3) / 1e9, 1),
+                             "data_gibs": round(3 * n * k * size / (med / 1e3) / 2**30, 1)}
+        del g
+    except Exception as e:  # reported, not fatal: the per-operation figures stand
+        out["step_graph"] = {"error": str(e)[:200]}
     # The timed launches rewrote parity and the erased shards: still the same bytes.
     out["mismatched_bytes"] += int((buf != orig).sum()) + int((~ver.verify_result()).sum())
     out["bit_exact"] = out["mismatched_bytes"] == 0
