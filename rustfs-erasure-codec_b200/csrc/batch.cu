@@ -166,10 +166,10 @@ __global__ void __launch_bounds__(kMixThreads, kMixBlocks) k_mix(MixArgs a) {
       switch (kind) {
         case MK_LEO8_ENC: fft_encode_tile<8, false, kMixThreads>(W, s_leo, jd, col0, job.len, &s_bad); break;
         case MK_LEO8_VERIFY: fft_encode_tile<8, true, kMixThreads>(W, s_leo, jd, col0, job.len, &s_bad); break;
-        case MK_LEO8_DEC: fft_decode_tile<8, kMixThreads>(W, s_leo, jd, col0, job.len); break;
+        case MK_LEO8_DEC: fft_decode_tile<8, kMixThreads, false>(W, s_leo, jd, col0, job.len); break;
         case MK_LEO16_ENC: fft_encode_tile<16, false, kMixThreads>(W, s_leo, jd, col0, job.len, &s_bad); break;
         case MK_LEO16_VERIFY: fft_encode_tile<16, true, kMixThreads>(W, s_leo, jd, col0, job.len, &s_bad); break;
-        default: fft_decode_tile<16, kMixThreads>(W, s_leo, jd, col0, job.len); break;
+        default: fft_decode_tile<16, kMixThreads, false>(W, s_leo, jd, col0, job.len); break;
       }
     }
     __syncthreads();  // every thread is done with s_item / s_leo before the next grab

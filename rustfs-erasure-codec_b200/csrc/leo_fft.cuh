@@ -357,11 +357,65 @@ __device__ __forceinline__ void smem_stage(uint32_t *S, uint32_t C, uint32_t lgC
   }
 }
 
-// Formal derivative over n lanes in shared memory (rows of C words), in
-// place.  New lane l depends only on old lanes above it, so each round reads
-// every value it needs, waits for the whole CTA, then writes.
+// Formal derivative over n >= 32 lanes held as rows of C >= 32 words (shared
+// memory, or the global work rows), in place: lane l gains the XOR of the old
+// lanes l | 2^t over the zero bits t of l (src/core/leopard_gf16/decode.rs:
+// 1100-1116, restated without the in-place sequencing).  A warp takes one
+// group of 16 consecutive lanes of a 32-word slice per round, as the stages
+// do: bits 0-3 come from its own 16 registers (lane j's sources are lanes
+// above j, so an ascending in-place pass reads only old values), and each
+// zero bit t >= 4 of the group's base adds the 16 lanes 2^t above it, 16
+// independent loads.  New lane l depends only on old lanes above it, and the
+// groups are taken in ascending order, so each round reads everything it
+// needs, waits for the whole CTA, then writes.
 template <int NT>
 __device__ void smem_derivative(uint32_t *S, uint32_t C, uint32_t lgC, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lgC32 = lgC - 5, lgn = 31 - __clz(n);
+  const uint32_t items = (n >> 4) << lgC32;
+  for (uint32_t r0 = 0; r0 < items; r0 += NT / 32) {
+    const uint32_t it = r0 + warp;
+    const bool have = it < items;  // warp-uniform
+    uint32_t v[16];
+    uint32_t *base = S;
+    if (have) {
+      const uint32_t R = (it >> lgC32) << 4;
+      base = S + size_t(R) * C + ((it & ((1u << lgC32) - 1)) << 5) + lane;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[j] = base[size_t(j) * C];
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+#pragma unroll
+        for (int t = 1; t < 16; t <<= 1)
+          if (!(j & t)) v[j] ^= v[j | t];
+      for (uint32_t t = 4; t < lgn; ++t) {
+        if (R & (1u << t)) continue;  // warp-uniform
+        const uint32_t *src = base + (size_t(1) << t) * C;
+#pragma unroll
+        for (int h = 0; h < 16; h += 8) {  // eight loads in flight at a time (register cap)
+          uint32_t u[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) u[j] = src[size_t(h + j) * C];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v[h + j] ^= u[j];
+        }
+      }
+    }
+    __syncthreads();
+    if (have) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) base[size_t(j) * C] = v[j];
+    }
+    __syncthreads();
+  }
+}
+
+// The same derivative one word per thread, up to kHold words per round: the
+// form the mixed kernel keeps (its K1 tiles share the kernel's 80 registers,
+// and the grouped form's 16-lane registers made the whole kernel spill more:
+// the mixed workload 2.7% slower).
+template <int NT>
+__device__ void flat_derivative(uint32_t *S, uint32_t C, uint32_t lgC, uint32_t n) {
   constexpr int kHold = 8;
   const uint32_t total = n << lgC;
   for (uint32_t base = 0; base < total; base += NT * kHold) {
@@ -746,7 +800,9 @@ __device__ __forceinline__ void dec_regs(const LeoArgs &a, const LeoJob &jd, con
 // below m + k), scale targets by mod - locator.
 // n <= 16: registers only, tile = 4 NT bytes.  n >= 32: W holds n rows of
 // C = 16 * a.nb words, tile = 4C bytes.
-template <int BITS, int NT>
+// GROUPED: the formal derivative by 16-lane groups (smem_derivative) or one
+// word per thread (flat_derivative; the mixed kernel's choice).
+template <int BITS, int NT, bool GROUPED = true>
 __device__ void fft_decode_tile(uint32_t *W, const LeoArgs &a, const LeoJob &jd, uint64_t col0, uint64_t len) {
   const uint32_t lane = threadIdx.x & 31;
   const FftCtx x{a.kbank, a.mod, lane, a.skew, a.sktab};
@@ -766,7 +822,10 @@ __device__ void fft_decode_tile(uint32_t *W, const LeoArgs &a, const LeoJob &jd,
     smem_stage<BITS, false, NT>(S, C, lgC32, n, st_at(a.st_idec, s), x, skd, jd.input_count);
     __syncthreads();
   }
-  smem_derivative<NT>(S, C, lgC, n);
+  if (GROUPED)
+    smem_derivative<NT>(S, C, lgC, n);
+  else
+    flat_derivative<NT>(S, C, lgC, n);
   for (uint32_t s = 0; s + 1 < a.n_fdec; ++s) {
     smem_stage<BITS, true, NT>(S, C, lgC32, n, st_at(a.st_fdec, s), x, skd, a.m + a.k);
     __syncthreads();
